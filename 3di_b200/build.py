@@ -1,0 +1,44 @@
+"""Builds the sm_100a shared library of the fitting path (libtdi_b200.so) in this directory."""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libtdi_b200.so")
+SOURCES = [os.path.join(HERE, "csrc", "tdi_api.cu")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("tdi_kernels.cu", "tdi_internal.cuh")] + [
+    os.path.join(HERE, "..", "include", "tdi.h")]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+    # formulas are restated operation by operation: no FMA contraction, IEEE div/sqrt
+    "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
+    "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
+]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.sep not in cand or os.path.exists(cand)):
+            return cand
+    return "nvcc"
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(p) <= t for p in DEPS)
+
+
+def build(force: bool = False, verbose: bool = False, extra=()) -> str:
+    if force or not up_to_date():
+        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", LIB, *SOURCES]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True,
+          extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else [])

@@ -1,0 +1,714 @@
+// C ABI and host driver of the batched 3DI fitting path (include/tdi.h).
+//
+// One batch fits F frames together. Each fitting stage (light fit, shape fit, finetune) is
+// a loop of rounds; in a round every frame still running the stage evaluates one point --
+// the start of a Gauss-Newton iteration or a line-search trial -- and a per-frame state
+// machine on the device applies the reference's decision rules. A frame whose trial is
+// accepted gets its normal equations in the same round: the accepted trial's render is the
+// render the next outer iteration of the reference would redo at the same point.
+#include "tdi_kernels.cu"
+
+#include "../../include/tdi.h"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace tdi;
+
+namespace {
+
+thread_local std::string g_err;
+
+tdi_status fail(tdi_status s, const std::string &msg)
+{
+    g_err = msg;
+    return s;
+}
+
+#define TDI_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(TDI_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TDI_LAUNCH()                                                                       \
+    do {                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(TDI_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_));   \
+    } while (0)
+
+inline int round4(int v) { return (v + 3) & ~3; }
+
+// Blur of full crops (the target, video_fitter.cu:548-549): rows then columns, the
+// oracle's summation order.
+__global__ void k_blur_rows_full(const float *src, float *dst, Cfg c, int F)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)F * NPIX) return;
+    const size_t f = i / NPIX;
+    const int p = (int)(i - f * NPIX), x = p >> 8, y = p & 255;
+    const float *s = src + f * NPIX;
+    float acc = 0.0f;
+    for (int j = -KRAD; j <= KRAD; ++j) {
+        const int yy = y + j;
+        const float v = (yy >= 0 && yy < DIM) ? s[x * DIM + yy] : 0.0f;
+        acc = acc + c.taps[KRAD - j] * v;
+    }
+    dst[i] = acc;
+}
+
+__global__ void k_blur_cols_full(const float *src, float *dst, Cfg c, int F)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)F * NPIX) return;
+    const size_t f = i / NPIX;
+    const int p = (int)(i - f * NPIX), x = p >> 8, y = p & 255;
+    const float *s = src + f * NPIX;
+    float acc = 0.0f;
+    for (int j = -KRAD; j <= KRAD; ++j) {
+        const int xx = x + j;
+        const float v = (xx >= 0 && xx < DIM) ? s[xx * DIM + y] : 0.0f;
+        acc = acc + c.taps[KRAD - j] * v;
+    }
+    dst[i] = acc;
+}
+
+__global__ void k_set_render(DBatch b, int frame)
+{
+    for (int f = threadIdx.x; f < b.F; f += blockDim.x) b.ctl[f].render = (f == frame);
+}
+
+__global__ void k_scalars(DBatch b, double *out)   // [F][4]
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    const FrameCtl &c = b.ctl[f];
+    out[f * 4 + 0] = c.corr;
+    out[f * 4 + 1] = (double)c.obj_b;
+    out[f * 4 + 2] = (double)c.obj0;
+    out[f * 4 + 3] = (double)c.face_ok;
+}
+
+Cfg to_cfg(const tdi_fit_config &c)
+{
+    Cfg r;
+    r.max_iters_rigid = c.max_iters_rigid;
+    r.max_iters_finetune = c.max_iters_finetune;
+    r.twostage_illum = c.twostage_illum;
+    r.finetune = c.finetune;
+    r.niters_success = c.niters_success;
+    r.max_iters_lambda = c.max_iters_lambda;
+    r.ref_face_size = c.ref_face_size;
+    for (int i = 0; i < NTAPS; ++i) r.taps[i] = c.taps[i];
+    return r;
+}
+
+}  // namespace
+
+struct tdi_model {
+    DModel d{};
+    std::vector<void *> allocs;
+    int device = 0;
+};
+
+struct tdi_batch {
+    tdi_model *m = nullptr;
+    int cap = 0;
+    DBatch d{};
+    std::vector<void *> allocs;
+    float *target_raw = nullptr;   // [cap][NPIX] unblurred upload
+    float *ctrl_scratch = nullptr;
+    double *scalars = nullptr;     // [cap][4]
+    int *d_count = nullptr;
+    int *h_count = nullptr;        // pinned
+    int device = 0;
+    int64_t launches = 0;          // kernels launched by this batch
+    int prof_id = 0;               // kernel timed by tdi_batch_profile
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+};
+
+namespace {
+
+template <typename T>
+tdi_status dalloc(std::vector<void *> &list, T **p, size_t n)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+    if (e != cudaSuccess) return fail(TDI_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    list.push_back(q);
+    *p = static_cast<T *>(q);
+    return TDI_OK;
+}
+
+#define TDI_TRY(x)                        \
+    do {                                  \
+        tdi_status s_ = (x);              \
+        if (s_ != TDI_OK) return s_;      \
+    } while (0)
+
+// Launches a kernel of this batch: counts it and, when it is the kernel being profiled,
+// brackets it with CUDA events on its stream.
+template <typename... KArgs, typename... Args>
+tdi_status launch(tdi_batch *bt, int kid, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                  cudaStream_t s, Args... args)
+{
+    const bool prof = kid != 0 && bt->prof_id == kid;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        TDI_CUDA(cudaEventCreate(&e0));
+        TDI_CUDA(cudaEventCreate(&e1));
+        TDI_CUDA(cudaEventRecord(e0, s));
+    }
+    kern<<<grid, block, smem, s>>>(args...);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(TDI_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    bt->launches++;
+    if (prof) {
+        TDI_CUDA(cudaEventRecord(e1, s));
+        bt->prof_events.emplace_back(e0, e1);
+    }
+    return TDI_OK;
+}
+
+// Crop origin from rescaled landmarks (renderer.cu:580-598, padding on).
+void crop_origin(const float *xl, const float *yl, int32_t *x0, int32_t *y0)
+{
+    float xmin = xl[0], xmax = xl[0], ymin = yl[0], ymax = yl[0];
+    for (int i = 1; i < NL; ++i) {
+        xmin = xl[i] < xmin ? xl[i] : xmin; xmax = xl[i] > xmax ? xl[i] : xmax;
+        ymin = yl[i] < ymin ? yl[i] : ymin; ymax = yl[i] > ymax ? yl[i] : ymax;
+    }
+    const float xs = xmax - xmin, ys = ymax - ymin;
+    const float sz = xs > ys ? xs : ys;
+    const float fx = (float)((double)xmin - (double)sz / 1.5);
+    const float fy = (float)((double)ymin - (double)sz / 1.5);
+    *x0 = (int32_t)(uint16_t)(fx > 0.0f ? fx : 0.0f);
+    *y0 = (int32_t)(uint16_t)(fy > 0.0f ? fy : 0.0f);
+}
+
+float face_size_of(const float *xl, const float *yl)
+{
+    float xmin = xl[0], xmax = xl[0], ymin = yl[0], ymax = yl[0];
+    for (int i = 1; i < NL; ++i) {
+        xmin = xl[i] < xmin ? xl[i] : xmin; xmax = xl[i] > xmax ? xl[i] : xmax;
+        ymin = yl[i] < ymin ? yl[i] : ymin; ymax = yl[i] > ymax ? yl[i] : ymax;
+    }
+    const float xs = xmax - xmin, ys = ymax - ymin;
+    return xs > ys ? xs : ys;
+}
+
+
+tdi_status set_attrs()
+{
+    static bool done = false;
+    if (done) return TDI_OK;
+    TDI_CUDA(cudaFuncSetAttribute(k_render, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  RENDER_SMEM_FLOATS * (int)sizeof(float)));
+    TDI_CUDA(cudaFuncSetAttribute(k_neighbours, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t))));
+    TDI_CUDA(cudaFuncSetAttribute(k_vertex, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_barrier_full, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_normal_eq, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    done = true;
+    return TDI_OK;
+}
+
+struct Launch {
+    tdi_batch *bt;
+    const DModel &m;
+    const DBatch &b;
+    cudaStream_t s;
+    int F;
+    size_t smem_vertex() const { return (size_t)(3 * m.KP * 33 + VT_F * m.KP) * sizeof(float); }
+    size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
+    size_t smem_ne() const { return (size_t)(2 * NE_CHUNK * m.KTP + 2 * NE_CHUNK) * sizeof(float); }
+    size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
+    size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
+    dim3 fblocks() const { return dim3((F + 127) / 128); }
+};
+
+tdi_status geometry(const Launch &L, const Cfg &c, int stage)
+{
+    dim3 vg((L.m.V + VT_V - 1) / VT_V, (L.F + VT_F - 1) / VT_F);
+    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, 0, k_precheck, L.fblocks(), dim3(128), 0, L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, KID_RASTER, k_raster, dim3(L.F), dim3(1024), 0, L.s, L.m, L.b));
+    return TDI_OK;
+}
+
+tdi_status render(const Launch &L, const Cfg &c, int stage)
+{
+    return launch(L.bt, KID_RENDER, k_render, dim3(L.F), dim3(RENDER_THREADS),
+                  RENDER_SMEM_FLOATS * sizeof(float), L.s, L.m, L.b, c, stage);
+}
+
+tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
+{
+    TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.F), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
+    TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.F), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(L.F), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.F), dim3(256), L.smem_bar(), L.s, L.m, L.b,
+                   (int)(stage == ST_FINETUNE)));
+    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.F), dim3(128), L.smem_solve(), L.s, L.m, L.b, c, stage));
+    return TDI_OK;
+}
+
+tdi_status run_stage(tdi_batch *bt, const Cfg &c, int stage, cudaStream_t s)
+{
+    const DModel &m = bt->m->d;
+    const DBatch &b = bt->d;
+    Launch L{bt, m, b, s, b.F};
+    TDI_TRY(launch(bt, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, b, c, stage));
+    const long max_rounds = stage == ST_LAMBDA ? 8L * c.max_iters_lambda + 16
+                                               : 16L * (stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune) + 16;
+    for (long round = 0; round < max_rounds; ++round) {
+        TDI_TRY(launch(bt, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, b, stage));
+        if (stage == ST_LAMBDA) {
+            if (round == 0) {
+                TDI_TRY(geometry(L, c, stage));
+                TDI_TRY(launch(bt, KID_NEIGHBOURS, k_neighbours, dim3(L.F), dim3(1024), L.smem_neigh(), s, b, 1));
+            }
+            TDI_TRY(render(L, c, stage));
+            TDI_TRY(launch(bt, 0, k_decide_lambda, L.fblocks(), dim3(128), 0, s, m, b, c));
+            TDI_TRY(launch(bt, 0, k_lambda_jac, dim3(L.F), dim3(256), 0, s, m, b, c));
+        } else {
+            TDI_TRY(geometry(L, c, stage));
+            TDI_TRY(render(L, c, stage));
+            TDI_TRY(launch(bt, 0, k_decide_shape, L.fblocks(), dim3(128), 0, s, m, b, c, stage));
+            TDI_TRY(normal_equations(L, c, stage));
+        }
+        TDI_TRY(launch(bt, 0, k_count_active, dim3(1), dim3(256), 0, s, b, bt->d_count));
+        TDI_CUDA(cudaMemcpyAsync(bt->h_count, bt->d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+        TDI_CUDA(cudaStreamSynchronize(s));
+        if (*bt->h_count == 0) break;
+    }
+    return TDI_OK;
+}
+
+__global__ void k_fit_begin(DBatch b)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &c = b.ctl[f];
+    c.flags = 0;
+    c.iters_rigid = c.iters_finetune = c.iters_lambda = 0;
+    c.renders = 0;
+    c.stage_ok = 0;
+    c.objective = 0.0f;
+    c.N = 0;
+}
+
+__global__ void k_fit_end(DBatch b)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &c = b.ctl[f];
+    if (!c.stage_ok) c.flags |= FLAG_FAIL;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tdi_last_error(void) { return g_err.c_str(); }
+
+tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
+{
+    if (!desc || !out) return fail(TDI_ERR_INVALID, "null argument");
+    const int V = desc->n_vertices, T = desc->n_triangles, K = desc->n_expr;
+    if (V <= 0 || T <= 0 || K <= 0 || K > 500 || !desc->mean || !desc->expr_basis || !desc->tex ||
+        !desc->triangles || !desc->landmarks || !desc->eps_lb || !desc->eps_ub ||
+        !desc->eps_lb_finetune || !desc->eps_ub_finetune)
+        return fail(TDI_ERR_INVALID, "incomplete model description");
+    if (T >= (1 << TRI_BITS)) return fail(TDI_ERR_INVALID, "too many triangles");
+    for (int i = 0; i < 3 * T; ++i)
+        if (desc->triangles[i] < 0 || desc->triangles[i] >= V) return fail(TDI_ERR_INVALID, "triangle index out of range");
+    for (int i = 0; i < NL; ++i)
+        if (desc->landmarks[i] < 0 || desc->landmarks[i] >= V) return fail(TDI_ERR_INVALID, "landmark index out of range");
+    TDI_TRY(set_attrs());
+    tdi_model *m = new tdi_model();
+    cudaGetDevice(&m->device);
+    DModel &d = m->d;
+    d.V = V; d.T = T; d.K = K; d.KP = round4(K); d.KT = K + 6; d.KTP = round4(K + 6);
+    float *mean, *E, *tex, *epsb;
+    int32_t *tl, *lis;
+    auto cleanup = [&](tdi_status st) { for (void *p : m->allocs) cudaFree(p); delete m; return st; };
+    tdi_status st;
+    if ((st = dalloc(m->allocs, &mean, 3 * (size_t)V)) || (st = dalloc(m->allocs, &E, (size_t)V * 3 * d.KP)) ||
+        (st = dalloc(m->allocs, &tex, (size_t)V)) || (st = dalloc(m->allocs, &tl, 3 * (size_t)T)) ||
+        (st = dalloc(m->allocs, &lis, (size_t)NL)) || (st = dalloc(m->allocs, &epsb, 4 * (size_t)K)))
+        return cleanup(st);
+    std::vector<float> Ep((size_t)V * 3 * d.KP, 0.0f);
+    for (size_t r = 0; r < (size_t)V * 3; ++r)
+        std::memcpy(&Ep[r * d.KP], desc->expr_basis + r * K, sizeof(float) * K);
+    std::vector<float> eb(4 * (size_t)K);
+    std::memcpy(&eb[0], desc->eps_lb, sizeof(float) * K);
+    std::memcpy(&eb[K], desc->eps_ub, sizeof(float) * K);
+    std::memcpy(&eb[2 * K], desc->eps_lb_finetune, sizeof(float) * K);
+    std::memcpy(&eb[3 * K], desc->eps_ub_finetune, sizeof(float) * K);
+    if (cudaMemcpy(mean, desc->mean, sizeof(float) * 3 * V, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(E, Ep.data(), sizeof(float) * Ep.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tex, desc->tex, sizeof(float) * V, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tl, desc->triangles, sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(lis, desc->landmarks, sizeof(int32_t) * NL, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(epsb, eb.data(), sizeof(float) * eb.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return cleanup(fail(TDI_ERR_CUDA, "model upload failed"));
+    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb;
+    *out = m;
+    return TDI_OK;
+}
+
+tdi_status tdi_model_destroy(tdi_model *m)
+{
+    if (!m) return TDI_OK;
+    for (void *p : m->allocs) cudaFree(p);
+    delete m;
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
+{
+    if (!m || !out || max_frames <= 0) return fail(TDI_ERR_INVALID, "bad batch arguments");
+    tdi_batch *b = new tdi_batch();
+    b->m = m;
+    b->cap = max_frames;
+    cudaGetDevice(&b->device);
+    const DModel &md = m->d;
+    DBatch &d = b->d;
+    const size_t F = (size_t)max_frames, KTP = md.KTP;
+    auto cleanup = [&](tdi_status st) {
+        for (void *p : b->allocs) cudaFree(p);
+        if (b->h_count) cudaFreeHost(b->h_count);
+        delete b;
+        return st;
+    };
+    float *target, *xl, *yl, *bounds, *fs, *cam, *Lint;
+    int32_t *x0y0;
+    tdi_status st = TDI_OK;
+#define A(ptr, n) if (st == TDI_OK) st = dalloc(b->allocs, &ptr, (n))
+    A(target, F * NPIX); A(b->target_raw, F * NPIX); A(xl, F * NL); A(yl, F * NL);
+    A(bounds, F * 4 * NL); A(fs, F); A(cam, F * 4); A(x0y0, F * 2); A(Lint, F);
+    A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
+    A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
+    A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
+    A(d.ctl, F); A(d.geo, F * 6 * md.V); A(d.zbuf, F * NPIX); A(d.frag, F * NMAX);
+    A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
+    A(d.J, F * NMAX * KTP); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
+    A(d.prof_frames, 1);
+#undef A
+    if (st != TDI_OK) return cleanup(st);
+    if (cudaMallocHost(&b->h_count, sizeof(int)) != cudaSuccess) return cleanup(fail(TDI_ERR_NOMEM, "pinned alloc"));
+    if (cudaMemset(d.zbuf, 0xFF, F * NPIX * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(d.ctl, 0, F * sizeof(FrameCtl)) != cudaSuccess ||
+        cudaMemset(d.x, 0, F * KTP * sizeof(float)) != cudaSuccess ||
+        cudaMemset(d.x_ls, 0, F * KTP * sizeof(float)) != cudaSuccess ||
+        cudaMemset(d.J, 0, F * NMAX * KTP * sizeof(float)) != cudaSuccess ||
+        cudaMemset(d.prof_frames, 0, sizeof(unsigned long long)) != cudaSuccess)
+        return cleanup(fail(TDI_ERR_CUDA, "batch init failed"));
+    d.F = max_frames;
+    d.target = target; d.xl = xl; d.yl = yl; d.bounds = bounds; d.face_size = fs; d.cam = cam;
+    d.x0y0 = x0y0; d.Lint = Lint;
+    d.prof_id = 0;
+    *out = b;
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_destroy(tdi_batch *b)
+{
+    if (!b) return TDI_OK;
+    for (auto &e : b->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    for (void *p : b->allocs) cudaFree(p);
+    if (b->h_count) cudaFreeHost(b->h_count);
+    delete b;
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *fr, void *stream)
+{
+    if (!b || !fr || !fr->targets || !fr->xl || !fr->yl || !fr->bounds || !fr->cam)
+        return fail(TDI_ERR_INVALID, "incomplete frames");
+    if (fr->n_frames <= 0) return fail(TDI_ERR_INVALID, "no frames");
+    if (fr->n_frames > b->cap) return fail(TDI_ERR_CAPACITY, "more frames than the batch holds");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int F = fr->n_frames;
+    b->d.F = F;
+    std::vector<int32_t> x0y0(2 * (size_t)F);
+    std::vector<float> fs(F);
+    for (int f = 0; f < F; ++f) {
+        if (fr->x0y0) { x0y0[2 * f] = fr->x0y0[2 * f]; x0y0[2 * f + 1] = fr->x0y0[2 * f + 1]; }
+        else crop_origin(fr->xl + f * NL, fr->yl + f * NL, &x0y0[2 * f], &x0y0[2 * f + 1]);
+        fs[f] = fr->face_size ? fr->face_size[f] : face_size_of(fr->xl + f * NL, fr->yl + f * NL);
+    }
+    DBatch &d = b->d;
+    TDI_CUDA(cudaMemcpyAsync(b->target_raw, fr->targets, sizeof(float) * NPIX * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)d.xl, fr->xl, sizeof(float) * NL * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)d.yl, fr->yl, sizeof(float) * NL * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)d.bounds, fr->bounds, sizeof(float) * 4 * NL * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)d.cam, fr->cam, sizeof(float) * 4 * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)d.x0y0, x0y0.data(), sizeof(int32_t) * 2 * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)d.face_size, fs.data(), sizeof(float) * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    return TDI_OK;
+}
+
+static tdi_status blur_targets(tdi_batch *b, const Cfg &c, cudaStream_t s)
+{
+    const size_t n = (size_t)b->d.F * NPIX;
+    const dim3 blocks((unsigned)((n + 255) / 256));
+    TDI_TRY(launch(b, 0, k_blur_rows_full, blocks, dim3(256), 0, s, (const float *)b->target_raw, b->d.img, c, b->d.F));
+    // img holds 2*NPIX floats per frame; the row pass above used the first F*NPIX floats
+    TDI_TRY(launch(b, 0, k_blur_cols_full, blocks, dim3(256), 0, s, (const float *)b->d.img, (float *)b->d.target, c, b->d.F));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_set_state(tdi_batch *b, const float *x, const float *lam, const float *L, void *stream)
+{
+    if (!b || !x || !lam || !L) return fail(TDI_ERR_INVALID, "null state");
+    cudaStream_t s = (cudaStream_t)stream;
+    const DModel &m = b->m->d;
+    const int F = b->d.F;
+    std::vector<float> xp((size_t)F * m.KTP, 0.0f), lp((size_t)F * 4, 0.0f);
+    for (int f = 0; f < F; ++f) {
+        std::memcpy(&xp[(size_t)f * m.KTP], x + (size_t)f * m.KT, sizeof(float) * m.KT);
+        for (int j = 0; j < 3; ++j) lp[f * 4 + j] = lam[f * 3 + j];
+    }
+    TDI_CUDA(cudaMemcpyAsync(b->d.x, xp.data(), sizeof(float) * xp.size(), cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync(b->d.x_ls, xp.data(), sizeof(float) * xp.size(), cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync(b->d.lam, lp.data(), sizeof(float) * lp.size(), cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync(b->d.lam_ls, lp.data(), sizeof(float) * lp.size(), cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaMemcpyAsync((void *)b->d.Lint, L, sizeof(float) * F, cudaMemcpyHostToDevice, s));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_fit(tdi_batch *b, const tdi_fit_config *cfg, void *stream)
+{
+    if (!b || !cfg) return fail(TDI_ERR_INVALID, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const Cfg c = to_cfg(*cfg);
+    const dim3 fb((b->d.F + 127) / 128);
+    TDI_TRY(blur_targets(b, c, s));
+    TDI_TRY(launch(b, 0, k_fit_begin, fb, dim3(128), 0, s, b->d));
+    TDI_TRY(run_stage(b, c, ST_LAMBDA, s));
+    TDI_TRY(run_stage(b, c, ST_RIGID, s));
+    if (c.twostage_illum) {
+        for (int k = 0; k < 2; ++k) {
+            TDI_TRY(run_stage(b, c, ST_LAMBDA, s));
+            TDI_TRY(run_stage(b, c, ST_RIGID, s));
+        }
+    }
+    if (c.finetune) TDI_TRY(run_stage(b, c, ST_FINETUNE, s));
+    TDI_TRY(launch(b, 0, k_fit_end, fb, dim3(128), 0, s, b->d));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_get_state(tdi_batch *b, float *x, float *lam, tdi_report *rep, void *stream)
+{
+    if (!b) return fail(TDI_ERR_INVALID, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    const DModel &m = b->m->d;
+    const int F = b->d.F;
+    std::vector<float> xp((size_t)F * m.KTP), lp((size_t)F * 4);
+    std::vector<FrameCtl> ctl(F);
+    TDI_CUDA(cudaMemcpyAsync(xp.data(), b->d.x, sizeof(float) * xp.size(), cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaMemcpyAsync(lp.data(), b->d.lam, sizeof(float) * lp.size(), cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaMemcpyAsync(ctl.data(), b->d.ctl, sizeof(FrameCtl) * F, cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    for (int f = 0; f < F; ++f) {
+        if (x) std::memcpy(x + (size_t)f * m.KT, &xp[(size_t)f * m.KTP], sizeof(float) * m.KT);
+        if (lam) for (int j = 0; j < 3; ++j) lam[f * 3 + j] = lp[f * 4 + j];
+        if (rep) {
+            rep[f].flags = ctl[f].flags;
+            rep[f].n_fragments = ctl[f].N;
+            rep[f].iters_rigid = ctl[f].iters_rigid;
+            rep[f].iters_finetune = ctl[f].iters_finetune;
+            rep[f].iters_lambda = ctl[f].iters_lambda;
+            rep[f].renders = ctl[f].renders;
+            rep[f].objective = ctl[f].objective;
+        }
+    }
+    return TDI_OK;
+}
+
+tdi_status tdi_fit_frames(tdi_batch *b, const tdi_frames *frames, const tdi_fit_config *cfg,
+                          float *x, float *lam, const float *L, tdi_report *rep, void *stream)
+{
+    TDI_TRY(tdi_batch_set_frames(b, frames, stream));
+    TDI_TRY(tdi_batch_set_state(b, x, lam, L, stream));
+    TDI_TRY(tdi_batch_fit(b, cfg, stream));
+    return tdi_batch_get_state(b, x, lam, rep, stream);
+}
+
+tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t finetune_bounds, void *stream)
+{
+    if (!b || !cfg) return fail(TDI_ERR_INVALID, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const Cfg c = to_cfg(*cfg);
+    const DModel &m = b->m->d;
+    const DBatch &d = b->d;
+    Launch L{b, m, d, s, d.F};
+    const int stage = finetune_bounds ? ST_FINETUNE : ST_RIGID;
+    TDI_TRY(blur_targets(b, c, s));
+    TDI_TRY(launch(b, 0, k_fit_begin, L.fblocks(), dim3(128), 0, s, d));
+    TDI_TRY(launch(b, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, d, c, stage));
+    TDI_TRY(launch(b, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, d, stage));
+    TDI_TRY(geometry(L, c, stage));
+    TDI_TRY(render(L, c, stage));
+    TDI_TRY(launch(b, 0, k_decide_shape, L.fblocks(), dim3(128), 0, s, m, d, c, stage));
+    TDI_TRY(normal_equations(L, c, stage));
+    TDI_TRY(launch(b, 0, k_scalars, L.fblocks(), dim3(128), 0, s, d, b->scalars));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, int64_t capacity, int64_t *count)
+{
+    if (!b || !dst || frame < 0 || frame >= b->d.F) return fail(TDI_ERR_INVALID, "bad read arguments");
+    const DModel &m = b->m->d;
+    const DBatch &d = b->d;
+    FrameCtl ctl;
+    TDI_CUDA(cudaDeviceSynchronize());
+    TDI_CUDA(cudaMemcpy(&ctl, d.ctl + frame, sizeof(FrameCtl), cudaMemcpyDeviceToHost));
+    const int64_t N = ctl.N;
+    int64_t n = 0;
+    auto copy_rows = [&](const void *src, size_t row_bytes, int rows, size_t src_pitch) -> tdi_status {
+        if ((int64_t)(row_bytes * rows) > capacity) return fail(TDI_ERR_INVALID, "destination too small");
+        TDI_CUDA(cudaMemcpy2D(dst, row_bytes, src, src_pitch, row_bytes, rows, cudaMemcpyDeviceToHost));
+        return TDI_OK;
+    };
+    switch (what) {
+    case 0:   // fragments: 16 bytes each
+        TDI_TRY(copy_rows(d.frag + (size_t)frame * NMAX, sizeof(Fragment) * N, 1, sizeof(Fragment) * NMAX));
+        n = N * 4;
+        break;
+    case 1:   // neighbours [4][N]
+        TDI_TRY(copy_rows(d.nb + (size_t)frame * 4 * NMAX, sizeof(int32_t) * N, 4, sizeof(int32_t) * NMAX));
+        n = N * 4;
+        break;
+    case 2:   // gradients [5][N]
+        TDI_TRY(copy_rows(d.fgrad + (size_t)frame * 5 * NMAX, sizeof(float) * N, 5, sizeof(float) * NMAX));
+        n = N * 5;
+        break;
+    case 3:   // jacobian [N][KT]
+        TDI_TRY(copy_rows(d.J + (size_t)frame * NMAX * m.KTP, sizeof(float) * m.KT, (int)N, sizeof(float) * m.KTP));
+        n = N * m.KT;
+        break;
+    case 4: { // H [KT][KT], g [KT], d [KT]
+        const int64_t need = (int64_t)(m.KT * m.KT + 2 * m.KT) * (int64_t)sizeof(float);
+        if (need > capacity) return fail(TDI_ERR_INVALID, "destination too small");
+        float *o = static_cast<float *>(dst);
+        TDI_CUDA(cudaMemcpy2D(o, sizeof(float) * m.KT, d.H + (size_t)frame * m.KTP * m.KTP, sizeof(float) * m.KTP,
+                              sizeof(float) * m.KT, m.KT, cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(o + m.KT * m.KT, d.g + (size_t)frame * m.KTP, sizeof(float) * m.KT, cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(o + m.KT * m.KT + m.KT, d.d + (size_t)frame * m.KTP, sizeof(float) * m.KT, cudaMemcpyDeviceToHost));
+        n = m.KT * m.KT + 2 * m.KT;
+        break;
+    }
+    case 5:
+        if (capacity < 4 * (int64_t)sizeof(double)) return fail(TDI_ERR_INVALID, "destination too small");
+        TDI_CUDA(cudaMemcpy(dst, b->scalars + (size_t)frame * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+        n = 4;
+        break;
+    case 6:
+        if (capacity < (int64_t)(6 * (size_t)m.V * sizeof(float))) return fail(TDI_ERR_INVALID, "destination too small");
+        TDI_CUDA(cudaMemcpy(dst, d.geo + (size_t)frame * 6 * m.V, 6 * (size_t)m.V * sizeof(float), cudaMemcpyDeviceToHost));
+        n = 6 * (int64_t)m.V;
+        break;
+    default:
+        return fail(TDI_ERR_INVALID, "unknown item");
+    }
+    if (count) *count = n;
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const float *yp, const float *zc,
+                            int32_t x0, int32_t y0, int32_t *n_out, uint32_t *flags_out)
+{
+    if (!b || !xp || !yp || !zc || frame < 0 || frame >= b->d.F) return fail(TDI_ERR_INVALID, "bad raster arguments");
+    const DModel &m = b->m->d;
+    DBatch &d = b->d;
+    float *g = d.geo + (size_t)frame * 6 * m.V;
+    TDI_CUDA(cudaMemcpy(g + 3 * (size_t)m.V, xp, sizeof(float) * m.V, cudaMemcpyHostToDevice));
+    TDI_CUDA(cudaMemcpy(g + 4 * (size_t)m.V, yp, sizeof(float) * m.V, cudaMemcpyHostToDevice));
+    TDI_CUDA(cudaMemcpy(g + 5 * (size_t)m.V, zc, sizeof(float) * m.V, cudaMemcpyHostToDevice));
+    int32_t o[2] = {x0, y0};
+    TDI_CUDA(cudaMemcpy((void *)(d.x0y0 + 2 * frame), o, sizeof(o), cudaMemcpyHostToDevice));
+    uint32_t zero = 0;
+    TDI_CUDA(cudaMemcpy(&d.ctl[frame].flags, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    TDI_TRY(launch(b, 0, k_set_render, dim3(1), dim3(256), 0, (cudaStream_t)0, d, (int)frame));
+    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(d.F), dim3(1024), 0, (cudaStream_t)0, m, d));
+    TDI_CUDA(cudaDeviceSynchronize());
+    FrameCtl ctl;
+    TDI_CUDA(cudaMemcpy(&ctl, d.ctl + frame, sizeof(FrameCtl), cudaMemcpyDeviceToHost));
+    if (n_out) *n_out = ctl.N;
+    if (flags_out) *flags_out = ctl.flags;
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void *stream)
+{
+    if (!b) return fail(TDI_ERR_INVALID, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    const DModel &m = b->m->d;
+    DBatch &d = b->d;
+    Launch L{b, m, d, s, d.F};
+    Cfg c{};
+    c.ref_face_size = 78.0f;
+    // evaluation point = x (shape-fit full evaluation), no fitting
+    TDI_TRY(launch(b, 0, k_fit_begin, L.fblocks(), dim3(128), 0, s, d));
+    TDI_TRY(launch(b, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, d, c, (int)ST_RIGID));
+    TDI_TRY(launch(b, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
+    dim3 vg((m.V + VT_V - 1) / VT_V, (d.F + VT_F - 1) / VT_F);
+    TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
+    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(d.F), dim3(1024), 0, s, m, d));
+    float *img = d.img;                                   // [F][NPIX] image, then [F][NPIX] map
+    int32_t *map = reinterpret_cast<int32_t *>(d.img + (size_t)d.F * NPIX);
+    TDI_TRY(launch(b, 0, k_paint, dim3(1, d.F), dim3(1024), 0, s, m, (const DBatch)d, img, map));
+    if (images) TDI_CUDA(cudaMemcpyAsync(images, img, sizeof(float) * NPIX * d.F, cudaMemcpyDeviceToHost, s));
+    if (tri_map) TDI_CUDA(cudaMemcpyAsync(tri_map, map, sizeof(int32_t) * NPIX * d.F, cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_launches(tdi_batch *b, int64_t *launches)
+{
+    if (!b || !launches) return fail(TDI_ERR_INVALID, "null argument");
+    *launches = b->launches;
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_profile(tdi_batch *b, int32_t kernel_id)
+{
+    if (!b || kernel_id < 0 || kernel_id > KID_SOLVE) return fail(TDI_ERR_INVALID, "bad kernel id");
+    for (auto &e : b->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    b->prof_events.clear();
+    b->prof_id = kernel_id;
+    b->d.prof_id = kernel_id;
+    TDI_CUDA(cudaMemset(b->d.prof_frames, 0, sizeof(unsigned long long)));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_profile_read(tdi_batch *b, int64_t *launches, double *total_ms, int64_t *frames)
+{
+    if (!b) return fail(TDI_ERR_INVALID, "null batch");
+    double ms = 0.0;
+    for (auto &e : b->prof_events) {
+        TDI_CUDA(cudaEventSynchronize(e.second));
+        float t = 0.0f;
+        TDI_CUDA(cudaEventElapsedTime(&t, e.first, e.second));
+        ms += t;
+    }
+    unsigned long long fr = 0;
+    TDI_CUDA(cudaMemcpy(&fr, b->d.prof_frames, sizeof(fr), cudaMemcpyDeviceToHost));
+    if (launches) *launches = (int64_t)b->prof_events.size();
+    if (total_ms) *total_ms = ms;
+    if (frames) *frames = (int64_t)fr;
+    return TDI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1458 @@
+// Kernels of the batched 3DI fitting path (sm_100a). Built with -fmad=false: every formula
+// below is evaluated in the operand order of the 3DI sources it restates, without FMA
+// contraction, so each per-fragment quantity is bit-identical to the CPU oracle's.
+#include "tdi_internal.cuh"
+
+#include <cfloat>
+#include <cmath>
+
+namespace tdi {
+
+// ------------------------------------------------------------------------------------------
+// Rotation R(u) and dR/du_i (rotation_header.cu:46-151).
+
+__device__ __forceinline__ void mul33(const float *A, const float *B, float *C)
+{
+    C[0] = (A[0] * B[0] + A[3] * B[1]) + A[6] * B[2];
+    C[1] = (A[1] * B[0] + A[4] * B[1]) + A[7] * B[2];
+    C[2] = (A[2] * B[0] + A[5] * B[1]) + A[8] * B[2];
+    C[3] = (A[0] * B[3] + A[3] * B[4]) + A[6] * B[5];
+    C[4] = (A[1] * B[3] + A[4] * B[4]) + A[7] * B[5];
+    C[5] = (A[2] * B[3] + A[5] * B[4]) + A[8] * B[5];
+    C[6] = (A[0] * B[6] + A[3] * B[7]) + A[6] * B[8];
+    C[7] = (A[1] * B[6] + A[4] * B[7]) + A[7] * B[8];
+    C[8] = (A[2] * B[6] + A[5] * B[7]) + A[8] * B[8];
+}
+
+__device__ __forceinline__ void skew(float *S, const float *u)
+{
+    S[0] = 0; S[1] = u[2]; S[2] = -u[1];
+    S[3] = -u[2]; S[4] = 0; S[5] = u[0];
+    S[6] = u[1]; S[7] = -u[0]; S[8] = 0;
+}
+
+__device__ void rotation(const float *u, float *R, float *dR)
+{
+    float theta = sqrtf((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
+    float un[3] = {u[0] / theta, u[1] / theta, u[2] / theta};
+    float R1[3][9], Sn[9], Sn2[9];
+    skew(R1[0], u); skew(R1[1], u); skew(R1[2], u);
+    skew(Sn, un);
+    float st = (float)sin((double)theta);
+    float cis = 1.0f - (float)cos((double)theta);
+    float tinv2 = 1.0f / (theta * theta);
+    for (int a = 0; a < 3; ++a)
+        for (int i = 0; i < 9; ++i) R1[a][i] *= u[a];
+    mul33(Sn, Sn, Sn2);
+    for (int i = 0; i < 9; ++i) {
+        if (i == 0 || i == 4 || i == 8)
+            R[i] = (cis * Sn2[i] + 1.0f) + st * Sn[i];
+        else
+            R[i] = cis * Sn2[i] + st * Sn[i];
+    }
+    float IR[9];
+    for (int i = 0; i < 9; ++i) IR[i] = R[i] * -1.0f;
+    IR[0] += 1; IR[4] += 1; IR[8] += 1;
+    for (int a = 0; a < 3; ++a) {
+        float R2[9], R3[9];
+        const float *c = IR + 3 * a;
+        R2[0] = u[0] * c[0]; R2[1] = u[0] * c[1]; R2[2] = u[0] * c[2];
+        R2[3] = u[1] * c[0]; R2[4] = u[1] * c[1]; R2[5] = u[1] * c[2];
+        R2[6] = u[2] * c[0]; R2[7] = u[2] * c[1]; R2[8] = u[2] * c[2];
+        for (int i = 0; i < 9; ++i) R1[a][i] += R2[i];
+        R3[0] = R1[a][0] - R2[0]; R3[1] = R1[a][1] - R2[3]; R3[2] = R1[a][2] - R2[6];
+        R3[3] = R1[a][3] - R2[1]; R3[4] = R1[a][4] - R2[4]; R3[5] = R1[a][5] - R2[7];
+        R3[6] = R1[a][6] - R2[2]; R3[7] = R1[a][7] - R2[5]; R3[8] = R1[a][8] - R2[8];
+        mul33(R3, R, dR + 9 * a);
+        for (int i = 0; i < 9; ++i) dR[9 * a + i] *= tinv2;
+    }
+}
+
+// Kernel ids for live profiling (tdi_batch_profile).
+enum KernelId : int32_t { KID_VERTEX = 1, KID_RASTER = 2, KID_RENDER = 3, KID_NEIGHBOURS = 4,
+                          KID_JACOBIAN = 5, KID_NORMAL_EQ = 6, KID_BARRIER = 7, KID_SOLVE = 8 };
+
+__device__ __forceinline__ void prof_count(const DBatch &b, int id, unsigned long long n = 1)
+{
+    if (b.prof_id == id) atomicAdd(b.prof_frames, n);
+}
+
+// ------------------------------------------------------------------------------------------
+// Stage control.
+
+__device__ __forceinline__ bool shape_stage(int stage) { return stage != ST_LAMBDA; }
+
+// Writes x_ls = x + t*d over the first n_upd entries; returns false when tau_z < 0 (the
+// reference's line search then breaks without terminating, and every later outer
+// iteration repeats the same trial: the frame is stuck at x, model_fitter.cu:255-259).
+__device__ bool set_trial(const DModel &m, const DBatch &b, int f, int n_upd)
+{
+    const float *x = b.x + (size_t)f * m.KTP;
+    const float *d = b.d + (size_t)f * m.KTP;
+    float *xl = b.x_ls + (size_t)f * m.KTP;
+    const float t = b.ctl[f].t;
+    for (int a = 0; a < n_upd; ++a) xl[a] = x[a] + t * d[a];
+    return !(xl[m.K + 2] < 0.0f);
+}
+
+__device__ void end_shape_stage(const Cfg &c, FrameCtl &ctl, int stage, int outer)
+{
+    ctl.active = 0;
+    ctl.render = 0;
+    ctl.need_jac = 0;
+    if (stage == ST_RIGID) ctl.iters_rigid += outer; else ctl.iters_finetune += outer;
+    if (stage == ST_RIGID) ctl.stage_ok = outer > c.niters_success;
+}
+
+// Line-search rejection (model_fitter.cu:325-355): shrink t, stop below the threshold,
+// otherwise place the next trial.
+__device__ void shape_reject(const DModel &m, const DBatch &b, const Cfg &c, int f, int stage)
+{
+    FrameCtl &ctl = b.ctl[f];
+    const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
+    ctl.t = ctl.t * 0.8f;
+    if (ctl.t < 0.075f) {
+        end_shape_stage(c, ctl, stage, ctl.outer < maxit ? ctl.outer + 1 : ctl.outer);
+        return;
+    }
+    const int n_upd = stage == ST_FINETUNE ? m.K : m.KT;
+    if (!set_trial(m, b, f, n_upd)) {
+        ctl.flags |= FLAG_STUCK_NEG_TZ;
+        end_shape_stage(c, ctl, stage, maxit);
+    }
+}
+
+__global__ void k_stage_start(DModel m, DBatch b, Cfg c, int stage)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &ctl = b.ctl[f];
+    const bool dead = (ctl.flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) != 0;
+    ctl.active = dead ? 0 : 1;
+    ctl.mode = M_FULL;
+    ctl.render = 0;
+    ctl.need_jac = 0;
+    ctl.t = 1.0f;
+    ctl.inner = 0;
+    ctl.outer = 1;
+    if (stage == ST_LAMBDA) {
+        for (int j = 0; j < 3; ++j) b.lam_ls[f * 4 + j] = b.lam[f * 4 + j];
+    }
+    // fit_3DMM_lambdas copies ov.betas into ov_linesearch (model_fitter.cu:991) and so
+    // does fit_to_video_frame before each shape fit (video_fitter.cu:570-574); the
+    // finetune keeps the line-search state the last shape fit left.
+    if (stage == ST_RIGID || stage == ST_LAMBDA) {
+        for (int a = 0; a < m.KT; ++a) b.x_ls[(size_t)f * m.KTP + a] = b.x[(size_t)f * m.KTP + a];
+    }
+}
+
+// Evaluation point, rotation and render flag of every active frame.
+__global__ void k_prepare(DModel m, DBatch b, int stage)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &ctl = b.ctl[f];
+    ctl.need_jac = 0;
+    if (!ctl.active) { ctl.render = 0; return; }
+    const float *src = (ctl.mode == M_FULL || stage == ST_LAMBDA) ? b.x : b.x_ls;
+    float *xe = b.xe + (size_t)f * m.KTP;
+    for (int a = 0; a < m.KT; ++a) xe[a] = src[(size_t)f * m.KTP + a];
+    rotation(xe + m.K + 3, b.R + f * 9, b.dR + f * 27);
+    ctl.render = 1;
+}
+
+// ------------------------------------------------------------------------------------------
+// Vertex stage: X0 = mean + E*eps (sequential fmaf over k), camera transform and
+// projection (renderer.cu:806-861, funcs.cu:395-453) for a tile of 32 vertices x 32 frames.
+// geo[f] = [X0 | Y0 | Z0 | xp | yp | Zc] planes of V floats.
+
+constexpr int VT_V = 32, VT_F = 32, VT_FPT = 4;   // vertices, frames per block; frames per thread
+
+__global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
+{
+    extern __shared__ float vsm[];
+    const int KP = m.KP, K = m.K;
+    float *Es = vsm;                           // [3*KP][33]
+    float *Xs = vsm + 3 * KP * 33;             // [VT_F][KP]
+    __shared__ int s_any;
+    const int v0 = blockIdx.x * VT_V, f0 = blockIdx.y * VT_F;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid == 0) s_any = 0;
+    __syncthreads();
+    if (tid < VT_F && f0 + tid < b.F && b.ctl[f0 + tid].render) {
+        s_any = 1;
+        if (blockIdx.x == 0) prof_count(b, KID_VERTEX);
+    }
+    __syncthreads();
+    if (!s_any) return;
+    const int nv = min(VT_V, m.V - v0);
+    for (int i = tid; i < VT_V * 3 * KP; i += 256) {
+        int vl = i / (3 * KP), rem = i - vl * 3 * KP;
+        Es[rem * 33 + vl] = vl < nv ? m.E[(size_t)(v0 + vl) * 3 * KP + rem] : 0.0f;
+    }
+    for (int i = tid; i < VT_F * KP; i += 256) {
+        int fl = i / KP, k = i - fl * KP;
+        int f = f0 + fl;
+        Xs[i] = (f < b.F && k < K) ? b.xe[(size_t)f * m.KTP + k] : 0.0f;
+    }
+    __syncthreads();
+    const int vl = threadIdx.x;
+    const int v = v0 + vl;
+    float acc[VT_FPT][3];
+#pragma unroll
+    for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
+    const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
+    for (int k = 0; k < K; ++k) {
+        const float ex = Es[(0 * KP + k) * 33 + vl];
+        const float ey = Es[(1 * KP + k) * 33 + vl];
+        const float ez = Es[(2 * KP + k) * 33 + vl];
+#pragma unroll
+        for (int q = 0; q < VT_FPT; ++q) {
+            const float e = xr[q * KP + k];
+            acc[q][0] = fmaf(ex, e, acc[q][0]);
+            acc[q][1] = fmaf(ey, e, acc[q][1]);
+            acc[q][2] = fmaf(ez, e, acc[q][2]);
+        }
+    }
+    if (v >= m.V) return;
+    const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
+#pragma unroll
+    for (int q = 0; q < VT_FPT; ++q) {
+        const int f = f0 + threadIdx.y * VT_FPT + q;
+        if (f >= b.F || !b.ctl[f].render) continue;
+        const float *R = b.R + f * 9;
+        const float *tau = b.xe + (size_t)f * m.KTP + K;
+        const float *cam = b.cam + f * 4;
+        const float X0 = mx + acc[q][0], Y0 = my + acc[q][1], Z0 = mz + acc[q][2];
+        const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
+        const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
+        const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
+        float *g = b.geo + (size_t)f * 6 * m.V;
+        g[v] = X0;
+        g[m.V + v] = Y0;
+        g[2 * m.V + v] = Z0;
+        g[3 * m.V + v] = (cam[0] * X3) / Z3 + cam[2];
+        g[4 * m.V + v] = (cam[1] * Y3) / Z3 + cam[3];
+        g[5 * m.V + v] = Z3;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Barrier objective of a state (logbarrier_initializer.cu:1921-2093 with compute_Gs :456-520):
+// expression bounds, then the four landmark box constraints. Landmark 3D points are the
+// vertex-stage object coordinates at the landmark vertices (same formula as the reference's
+// p0L + EL*eps). Sequential FP64 sum in the oracle's order.
+
+__device__ double barrier_objective(const DModel &m, const DBatch &b, int f, int ft_bounds,
+                                    float G[4][NL])
+{
+    const float *x = b.xe + (size_t)f * m.KTP;
+    const float *R = b.R + f * 9;
+    const float *tau = x + m.K;
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *lb = m.eps_b + (ft_bounds ? 2 : 0) * m.K;
+    const float *ub = m.eps_b + (ft_bounds ? 3 : 1) * m.K;
+    const float *cam = b.cam + f * 4;
+    const float phix = cam[0], phiy = cam[1], cx = cam[2], cy = cam[3];
+    const float fs = b.face_size[f];
+    const float *bnd = b.bounds + (size_t)f * 4 * NL;
+    const float *xl = b.xl + f * NL, *yl = b.yl + f * NL;
+    double obj = 0.0;
+    for (int k = 0; k < m.K; ++k) {
+        float fub = x[k] - ub[k];
+        float flb = lb[k] - x[k];
+        obj += (double)(-(float)log((double)(-flb)));
+        obj += (double)(-(float)log((double)(-fub)));
+    }
+    for (int i = 0; i < NL; ++i) {
+        const int v = m.lis[i];
+        const float p0 = geo[v], p1 = geo[m.V + v], p2 = geo[2 * m.V + v];
+        const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
+        const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
+        const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
+        const float xproj = phix * ((r1p + tau[0]) / (r3p + tau[2])) + cx;
+        const float yproj = phiy * ((r2p + tau[1]) / (r3p + tau[2])) + cy;
+        G[0][i] = 0.0f - ((xl[i] + bnd[0 * NL + i] * fs) - xproj);
+        G[1][i] = 0.0f - ((yl[i] + bnd[1 * NL + i] * fs) - yproj);
+        G[2][i] = 0.0f - ((xproj - bnd[2 * NL + i] * fs) - xl[i]);
+        G[3][i] = 0.0f - ((yproj - bnd[3 * NL + i] * fs) - yl[i]);
+    }
+    for (int s = 0; s < 4; ++s)
+        for (int i = 0; i < NL; ++i) obj += (double)(-(float)log((double)G[s][i]));
+    return obj;
+}
+
+// Face-size check (renderer.cu:838-857), barrier objective and the pre-render decisions of
+// a trial (model_fitter.cu:237-300): tau_z, face size, NaN barrier, then -g.d < 3e-4.
+__global__ void k_precheck(DModel m, DBatch b, Cfg c, int stage)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.active || !ctl.render) return;
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *xp = geo + 3 * m.V, *yp = geo + 4 * m.V;
+    const int *L = m.lis;
+    const float d_iod = fabsf(xp[L[9]] - xp[L[0]]);
+    const float d_lem = fabsf(yp[L[0]] - yp[L[40]]);
+    const float d_rem = fabsf(yp[L[9]] - yp[L[40]]);
+    const double lim = (double)c.ref_face_size * 2;
+    const int face_ok = !((double)d_iod > lim || (double)d_lem > lim || (double)d_rem > lim);
+    ctl.face_ok = face_ok;
+    if (!shape_stage(stage)) return;
+    float G[4][NL];
+    const double ob = barrier_objective(m, b, f, stage == ST_FINETUNE, G);
+    ctl.obj_b = (float)ob;
+    if (ctl.mode != M_TRIAL) return;
+    if (!face_ok || isnan(ob)) {
+        ctl.render = 0;
+        shape_reject(m, b, c, f, stage);
+        return;
+    }
+    if ((double)(-ctl.l2base) < 0.0003) {
+        ctl.render = 0;
+        const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
+        end_shape_stage(c, ctl, stage, ctl.outer < maxit ? ctl.outer + 1 : ctl.outer);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Visibility: one 1024-thread block per frame (get_pixels_to_render + keep_only_minZ +
+// remove_if, funcs.cu:900-1029, renderer.cu:650-680). Pass A enumerates each triangle's
+// <= 4 fragments in bounding-box order and folds a 64-bit key
+// [epoch tag | depth bits | triangle id] into the frame's z-buffer with atomicMin; pass B
+// counts survivors (depth equal to the pixel minimum) per slot row and warp; pass C writes
+// them in slot order (row-major over r, then triangle). The pixel owner is the minimum key
+// (smallest triangle among depth ties). Slot 0 is dropped, as remove_if(is_zero) does.
+
+__device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, const float *yp,
+                                             int idx, int x0, int y0, uint16_t pix[NTMP],
+                                             float al[NTMP], float be[NTMP], uint32_t &flags)
+{
+    const int T = m.T;
+    const int ib = m.tl[idx], ic = m.tl[T + idx], ia = m.tl[2 * T + idx];
+    const float bx = xp[ib], cx = xp[ic], ax = xp[ia];
+    const float by = yp[ib], cy = yp[ic], ay = yp[ia];
+    const float xhi = ceilf(fmaxf(fmaxf(bx, cx), ax));
+    const float yhi = ceilf(fmaxf(fmaxf(by, cy), ay));
+    float xlo_f = floorf(fminf(fminf(bx, cx), ax));
+    float ylo_f = floorf(fminf(fminf(by, cy), ay));
+    if (!(xlo_f >= 0.0f) || !(ylo_f >= 0.0f) || xhi > 65535.0f || yhi > 65535.0f) {
+        flags |= FLAG_OUT_OF_DOMAIN;
+        if (!(xhi <= 65535.0f && yhi <= 65535.0f)) return 0;
+        xlo_f = xlo_f >= 0.0f ? xlo_f : 0.0f;
+        ylo_f = ylo_f >= 0.0f ? ylo_f : 0.0f;
+    }
+    // A triangle whose box spans millions of pixels only arises from a vertex near the camera
+    // plane; the reference would walk the whole box. It is skipped and flagged instead.
+    if ((xhi - xlo_f) * (yhi - ylo_f) > 4194304.0f) {
+        flags |= FLAG_OUT_OF_DOMAIN;
+        return 0;
+    }
+    const uint16_t xlo = (uint16_t)xlo_f, ylo = (uint16_t)ylo_f;
+    int ridx = 0;
+    for (uint16_t x = xlo; (float)x < xhi && ridx < NTMP; ++x) {
+        for (uint16_t y = ylo; (float)y < yhi && ridx < NTMP; ++y) {
+            float v0x = bx - ax, v1x = cx - ax, v2x = (float)x - ax;
+            float v0y = by - ay, v1y = cy - ay, v2y = (float)y - ay;
+            float d00 = v0x * v0x + v0y * v0y;
+            float d01 = v0x * v1x + v0y * v1y;
+            float d11 = v1x * v1x + v1y * v1y;
+            float d20 = v0x * v2x + v0y * v2y;
+            float d21 = v1x * v2x + v1y * v2y;
+            float denom = d00 * d11 - d01 * d01;
+            float alpha = (d11 * d20 - d01 * d21) / denom;
+            float beta = (d00 * d21 - d01 * d20) / denom;
+            if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
+                int px = ((int)y - y0) + ((int)x - x0) * DIM;
+                if (px < 0 || px >= NPIX) flags |= FLAG_OUT_OF_DOMAIN;
+                pix[ridx] = (uint16_t)px;
+                al[ridx] = alpha;
+                be[ridx] = beta;
+                ridx++;
+            }
+        }
+    }
+    return ridx;
+}
+
+__device__ __forceinline__ unsigned long long zkey(uint32_t tag, float Z, int tri)
+{
+    return ((unsigned long long)tag << (31 + TRI_BITS)) |
+           ((unsigned long long)(__float_as_uint(Z) & 0x7FFFFFFFu) << TRI_BITS) |
+           (unsigned long long)(uint32_t)tri;
+}
+
+__global__ void __launch_bounds__(1024) k_raster(DModel m, DBatch b)
+{
+    const int f = blockIdx.x;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.render) return;
+    if (threadIdx.x == 0) prof_count(b, KID_RASTER);
+    __shared__ uint32_t s_cnt[32][NTMP];
+    __shared__ uint32_t s_off[32][NTMP];
+    __shared__ int s_bbox[4];
+    __shared__ uint32_t s_flags;
+    __shared__ uint32_t s_tag;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned long long *zb = b.zbuf + (size_t)f * NPIX;
+    if (tid == 0) {
+        uint32_t e = ctl.epoch + 1;
+        if (e > TAG_MAX) e = 0;           // wrap: clear below, restart the epochs
+        s_tag = e;
+        s_flags = 0;
+        s_bbox[0] = s_bbox[2] = 1 << 30;
+        s_bbox[1] = s_bbox[3] = -1;
+    }
+    __syncthreads();
+    if (s_tag == 0) {
+        for (int p = tid; p < NPIX; p += 1024) zb[p] = ~0ull;
+        __syncthreads();
+        if (tid == 0) s_tag = 1;
+        __syncthreads();
+    }
+    const uint32_t epoch = s_tag;
+    const uint32_t tag = TAG_MAX - epoch;
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *xp = geo + 3 * m.V, *yp = geo + 4 * m.V, *Zc = geo + 5 * m.V;
+    const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
+    const int T = m.T;
+    const int per_warp = ((T + 32 * 32 - 1) / (32 * 32)) * 32;
+    const int t_begin = warp * per_warp;
+    const int t_end = min(T, t_begin + per_warp);
+    uint32_t flags = 0;
+    int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
+
+    // pass A: depth keys
+    for (int base = t_begin; base < t_end; base += 32) {
+        const int idx = base + lane;
+        if (idx < t_end) {
+            uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
+            const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, flags);
+            if (nf) {
+                const float Z = Zc[m.tl[idx]];
+                if (!(Z > 0.0f)) flags |= FLAG_OUT_OF_DOMAIN;
+                const unsigned long long key = zkey(tag, Z, idx);
+                for (int r = 0; r < nf; ++r) atomicMin(zb + pix[r], key);
+            }
+        }
+    }
+    __syncthreads();
+
+    // pass B: survivors per slot row
+    uint32_t cnt[NTMP] = {0, 0, 0, 0};
+    for (int base = t_begin; base < t_end; base += 32) {
+        const int idx = base + lane;
+        bool s[NTMP] = {false, false, false, false};
+        if (idx < t_end) {
+            uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
+            uint32_t fl2 = 0;
+            const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
+            if (nf) {
+                const float Z = Zc[m.tl[idx]];
+                const uint32_t zb_bits = __float_as_uint(Z) & 0x7FFFFFFFu;
+                for (int r = 0; r < nf; ++r) {
+                    const unsigned long long k = __ldcg(zb + pix[r]);
+                    const bool live = (uint32_t)(k >> (31 + TRI_BITS)) == tag &&
+                                      (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zb_bits;
+                    s[r] = live && !(r == 0 && idx == 0);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, s[r]));
+    }
+    if (lane == 0)
+        for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
+    __syncthreads();
+    if (tid < NTMP) {
+        // exclusive scan over warps for row r; rows follow each other
+        uint32_t tot = 0;
+        for (int w = 0; w < 32; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
+        s_cnt[0][tid] = tot;     // reuse: row totals (read after the barrier below)
+    }
+    __syncthreads();
+    uint32_t rowbase[NTMP];
+    {
+        uint32_t acc = 0;
+        for (int r = 0; r < NTMP; ++r) { rowbase[r] = acc; acc += s_cnt[0][r]; }
+        if (tid == 0) {
+            ctl.N = (int)min(acc, (uint32_t)NMAX);
+            if (acc > (uint32_t)NMAX) atomicOr(&s_flags, FLAG_OVERFLOW);
+            if (acc < 1000u || acc > 52000u) atomicOr(&s_flags, FLAG_RENDER_SKIPPED);
+            if (acc > 25600u) atomicOr(&s_flags, FLAG_OUT_OF_DOMAIN);
+        }
+    }
+
+    // pass C: write survivors in slot order
+    uint32_t run[NTMP] = {0, 0, 0, 0};
+    const unsigned lt_mask = (1u << lane) - 1u;
+    Fragment *out = b.frag + (size_t)f * NMAX;
+    for (int base = t_begin; base < t_end; base += 32) {
+        const int idx = base + lane;
+        bool s[NTMP] = {false, false, false, false};
+        bool own[NTMP] = {false, false, false, false};
+        uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
+        int nf = 0;
+        if (idx < t_end) {
+            uint32_t fl2 = 0;
+            nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
+            if (nf) {
+                const float Z = Zc[m.tl[idx]];
+                const uint32_t zb_bits = __float_as_uint(Z) & 0x7FFFFFFFu;
+                const unsigned long long mykey = zkey(tag, Z, idx);
+                for (int r = 0; r < nf; ++r) {
+                    const unsigned long long k = __ldcg(zb + pix[r]);
+                    const bool live = (uint32_t)(k >> (31 + TRI_BITS)) == tag &&
+                                      (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zb_bits;
+                    s[r] = live && !(r == 0 && idx == 0);
+                    own[r] = (k == mykey);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NTMP; ++r) {
+            const unsigned mask = __ballot_sync(0xffffffffu, s[r]);
+            if (s[r]) {
+                const uint32_t pos = rowbase[r] + s_off[warp][r] + run[r] + __popc(mask & lt_mask);
+                if (pos < (uint32_t)NMAX) {
+                    Fragment fr;
+                    fr.pix_owner = (uint32_t)pix[r] | (own[r] ? 0x80000000u : 0u);
+                    fr.tri = idx;
+                    fr.al = al[r];
+                    fr.be = be[r];
+                    out[pos] = fr;
+                }
+                const int px = pix[r] >> 8, py = pix[r] & 255;
+                bx0 = min(bx0, px); bx1 = max(bx1, px);
+                by0 = min(by0, py); by1 = max(by1, py);
+            }
+            run[r] += __popc(mask);
+        }
+    }
+    if (flags) atomicOr(&s_flags, flags);
+    if (bx1 >= 0) {
+        atomicMin(&s_bbox[0], bx0); atomicMax(&s_bbox[1], bx1);
+        atomicMin(&s_bbox[2], by0); atomicMax(&s_bbox[3], by1);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        ctl.epoch = epoch;
+        ctl.flags |= s_flags;
+        ctl.renders += 1;
+        for (int q = 0; q < 4; ++q) ctl.bbox[q] = s_bbox[q];
+        if (s_bbox[1] >= 0 && (s_bbox[0] < 1 || s_bbox[1] > DIM - 2 || s_bbox[2] < 1 || s_bbox[3] > DIM - 2))
+            ctl.flags |= FLAG_OUT_OF_DOMAIN;
+        if (s_flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) ctl.render = 0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Render of one frame from its fragments, one block per frame: shading
+// (fill_diffuse_component_and_populate_texture_and_shape, newfuncs.cu:18-167), owners
+// painted into a zeroed image (fill_tex_im1, funcs.cu:800-817), the 15-tap separable blur
+// (newfuncs.cu:539-715) over the fragment box plus its 8-pixel margin (the image is zero
+// outside that box, so the result equals the full-image blur there), then the
+// normalised gradients of render and target at every fragment (fill_grads, funcs.cu:842-897)
+// and the correlation sum.
+
+struct Shading {
+    float tex, Id, nn[3], p[3], v[3];
+};
+
+__device__ __forceinline__ void camera_coords(const float *R, const float *tau, float X0, float Y0,
+                                              float Z0, float &X, float &Y, float &Z)
+{
+    X = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
+    Y = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
+    Z = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
+}
+
+__device__ __forceinline__ Shading shade(const DModel &m, const float *geo, const Fragment &fr,
+                                         const float *R, const float *tau, const float *lam,
+                                         float Lint)
+{
+    const int V = m.V, T = m.T, tri = fr.tri;
+    const int ib = m.tl[tri], ic = m.tl[T + tri], ia = m.tl[2 * T + tri];
+    const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
+    const float b0x = geo[ib], b0y = geo[V + ib], b0z = geo[2 * V + ib];
+    const float c0x = geo[ic], c0y = geo[V + ic], c0z = geo[2 * V + ic];
+    const float a0x = geo[ia], a0y = geo[V + ia], a0z = geo[2 * V + ia];
+    const float n_vx = b0x - a0x, n_vy = b0y - a0y, n_vz = b0z - a0z;
+    const float n_wx = c0x - a0x, n_wy = c0y - a0y, n_wz = c0z - a0z;
+    const float nrx = n_vy * n_wz - n_vz * n_wy;
+    const float nry = n_vz * n_wx - n_vx * n_wz;
+    const float nrz = n_vx * n_wy - n_vy * n_wx;
+    const float normn = sqrtf((nrx * nrx + nry * nry) + nrz * nrz);
+    Shading s;
+    s.nn[0] = nrx / normn; s.nn[1] = nry / normn; s.nn[2] = nrz / normn;
+    s.p[0] = (b0x * al + c0x * be) + a0x * ga;
+    s.p[1] = (b0y * al + c0y * be) + a0y * ga;
+    s.p[2] = (b0z * al + c0z * be) + a0z * ga;
+    const float d0 = lam[0] - tau[0], d1 = lam[1] - tau[1], d2 = lam[2] - tau[2];
+    float Id = (s.nn[0] * ((R[0] * d0 + R[1] * d1) + R[2] * d2)
+                + s.nn[1] * ((R[3] * d0 + R[4] * d1) + R[5] * d2))
+               + s.nn[2] * ((R[6] * d0 + R[7] * d1) + R[8] * d2);
+    Id = Id - ((s.nn[0] * s.p[0] + s.nn[1] * s.p[1]) + s.nn[2] * s.p[2]);
+    const float t = (m.tex[ib] * al + m.tex[ic] * be) + m.tex[ia] * ga;
+    s.tex = t + (Lint * t) * Id;
+    s.Id = Id;
+    float bX, bY, bZ, cX, cY, cZ, aX, aY, aZ;
+    camera_coords(R, tau, b0x, b0y, b0z, bX, bY, bZ);
+    camera_coords(R, tau, c0x, c0y, c0z, cX, cY, cZ);
+    camera_coords(R, tau, a0x, a0y, a0z, aX, aY, aZ);
+    s.v[0] = (bX * al + cX * be) + aX * ga;
+    s.v[1] = (bY * al + cY * be) + aY * ga;
+    s.v[2] = (bZ * al + cZ * be) + aZ * ga;
+    return s;
+}
+
+__device__ __forceinline__ void pixel_grad(const float *im, int x, int y, int rx0, int ry0, int rh,
+                                           float &gx, float &gy, float &h, float &gxn, float &gyn)
+{
+    // neighbours as fill_grads forms them (index 0 past the crop border); the region holds
+    // every pixel these can name (the whole crop when the fragments touch its border)
+    const int kr = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
+    const int kl = (x > 0) ? (x - 1) * DIM + y : 0;
+    const int ka = (y > 0) ? x * DIM + y - 1 : 0;
+    const int kb = (y < DIM - 1) ? x * DIM + y + 1 : 0;
+    auto at = [&](int p) { return im[((p >> 8) - rx0) * rh + ((p & 255) - ry0)]; };
+    const float a = 0.5f * (at(kr) - at(kl));
+    const float bb = 0.5f * (at(kb) - at(ka));
+    const float hh = 1e-16f + sqrtf((4 * a) * a + (4 * bb) * bb);
+    gx = a; gy = bb; h = hh;
+    gxn = (2.0f * a) / hh;
+    gyn = (2.0f * bb) / hh;
+}
+
+__device__ __forceinline__ void target_grad(const float *im, int ks, float &gxn, float &gyn)
+{
+    const int y = ks & 255, x = ks >> 8;
+    const int kr = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
+    const int kl = (x > 0) ? (x - 1) * DIM + y : 0;
+    const int ka = (y > 0) ? x * DIM + y - 1 : 0;
+    const int kb = (y < DIM - 1) ? x * DIM + y + 1 : 0;
+    const float a = 0.5f * (im[kr] - im[kl]);
+    const float bb = 0.5f * (im[kb] - im[ka]);
+    const float hh = 1e-16f + sqrtf((4 * a) * a + (4 * bb) * bb);
+    gxn = (2.0f * a) / hh;
+    gyn = (2.0f * bb) / hh;
+}
+
+constexpr int RENDER_THREADS = 512;
+constexpr int RENDER_SMEM_FLOATS = 50 * 1024;   // two region buffers of up to 25,600 floats
+
+__global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, Cfg c, int stage)
+{
+    const int f = blockIdx.x;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.render) return;
+    if (threadIdx.x == 0) prof_count(b, KID_RENDER);
+    extern __shared__ float rsm[];
+    __shared__ double s_red[RENDER_THREADS / 32];
+    const int tid = threadIdx.x;
+    const int N = ctl.N;
+    const bool border = ctl.bbox[0] < 1 || ctl.bbox[1] > DIM - 2 || ctl.bbox[2] < 1 || ctl.bbox[3] > DIM - 2;
+    const int rx0 = border ? 0 : max(0, ctl.bbox[0] - 8), rx1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[1] + 8);
+    const int ry0 = border ? 0 : max(0, ctl.bbox[2] - 8), ry1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[3] + 8);
+    const int rw = rx1 - rx0 + 1, rh = ry1 - ry0 + 1;
+    const int area = rw * rh;
+    float *A, *B;
+    if (2 * area <= RENDER_SMEM_FLOATS) { A = rsm; B = rsm + area; }
+    else { A = b.img + (size_t)f * 2 * NPIX; B = A + NPIX; }
+    for (int i = tid; i < area; i += RENDER_THREADS) A[i] = 0.0f;
+    __syncthreads();
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *R = b.R + f * 9;
+    const float *xsrc = stage == ST_LAMBDA ? b.x : b.xe;
+    const float *tau = xsrc + (size_t)f * m.KTP + m.K;
+    const float *lam = (stage == ST_LAMBDA && ctl.mode == M_TRIAL) ? b.lam_ls + f * 4 : b.lam + f * 4;
+    const float Lint = b.Lint[f];
+    const Fragment *frags = b.frag + (size_t)f * NMAX;
+    for (int n = tid; n < N; n += RENDER_THREADS) {
+        const Fragment fr = frags[n];
+        if (fr.pix_owner & 0x80000000u) {
+            const Shading s = shade(m, geo, fr, R, tau, lam, Lint);
+            const int p = fr.pix_owner & 0xFFFF;
+            A[((p >> 8) - rx0) * rh + ((p & 255) - ry0)] = s.tex;
+        }
+    }
+    __syncthreads();
+    // rows: along the contiguous (y) index
+    for (int i = tid; i < area; i += RENDER_THREADS) {
+        const int xl = i / rh, yl = i - xl * rh;
+        float s = 0.0f;
+        for (int j = -KRAD; j <= KRAD; ++j) {
+            const int yy = yl + j;
+            const float v = (yy >= 0 && yy < rh) ? A[xl * rh + yy] : 0.0f;
+            s = s + c.taps[KRAD - j] * v;
+        }
+        B[i] = s;
+    }
+    __syncthreads();
+    // columns: along the strided (x) index
+    for (int i = tid; i < area; i += RENDER_THREADS) {
+        const int xl = i / rh, yl = i - xl * rh;
+        float s = 0.0f;
+        for (int j = -KRAD; j <= KRAD; ++j) {
+            const int xx = xl + j;
+            const float v = (xx >= 0 && xx < rw) ? B[xx * rh + yl] : 0.0f;
+            s = s + c.taps[KRAD - j] * v;
+        }
+        A[i] = s;
+    }
+    __syncthreads();
+    const float *tgt = b.target + (size_t)f * NPIX;
+    float *fg = b.fgrad + (size_t)f * 5 * NMAX;
+    double corr = 0.0;
+    for (int n = tid; n < N; n += RENDER_THREADS) {
+        const int p = frags[n].pix_owner & 0xFFFF;
+        const int x = p >> 8, y = p & 255;
+        float gx, gy, h, gxn, gyn, sxn, syn;
+        pixel_grad(A, x, y, rx0, ry0, rh, gx, gy, h, gxn, gyn);
+        target_grad(tgt, p, sxn, syn);
+        fg[n] = gx; fg[NMAX + n] = gy; fg[2 * NMAX + n] = h;
+        fg[3 * NMAX + n] = sxn; fg[4 * NMAX + n] = syn;
+        corr += (double)gxn * (double)sxn + (double)gyn * (double)syn;
+    }
+    for (int o = 16; o > 0; o >>= 1) corr += __shfl_down_sync(0xffffffffu, corr, o);
+    if ((tid & 31) == 0) s_red[tid >> 5] = corr;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < RENDER_THREADS / 32; ++w) s += s_red[w];
+        ctl.corr = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Decisions after a render.
+
+// Shape fits (model_fitter.cu:215-356): objective -(tau*corr - barrier); Armijo test.
+__global__ void k_decide_shape(DModel m, DBatch b, Cfg c, int stage)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.active) return;
+    const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
+    if (ctl.flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) {
+        end_shape_stage(c, ctl, stage, ctl.outer);
+        return;
+    }
+    if (!ctl.render) return;
+    const float tau_img = 5.0f * 5.0f;
+    float gc = tau_img * (float)ctl.corr;
+    gc = gc + (-ctl.obj_b);
+    const float obj = -gc;
+    if (ctl.mode == M_FULL) {
+        ctl.obj0 = obj;
+        ctl.objective = obj;
+        ctl.need_jac = 1;
+        return;
+    }
+    ctl.inner++;
+    float l2 = ctl.l2base;
+    l2 = l2 * (0.4f * ctl.t);
+    if (obj < ctl.obj0 + l2) {
+        for (int a = 0; a < m.KT; ++a) b.x[(size_t)f * m.KTP + a] = b.x_ls[(size_t)f * m.KTP + a];
+        ctl.obj0 = obj;
+        ctl.objective = obj;
+        if (ctl.outer >= maxit) { end_shape_stage(c, ctl, stage, ctl.outer); return; }
+        ctl.outer++;
+        ctl.need_jac = 1;
+    } else {
+        shape_reject(m, b, c, f, stage);
+    }
+}
+
+// Light fit (model_fitter.cu:981-1073): objective -corr; Armijo test with alpha = beta = 0.5.
+__global__ void k_decide_lambda(DModel m, DBatch b, Cfg c)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.F) return;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.active) return;
+    if (ctl.flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) { ctl.active = 0; return; }
+    if (!ctl.render) return;
+    const float obj = -(float)ctl.corr;
+    if (ctl.mode == M_FULL) {
+        ctl.obj0 = obj;
+        ctl.iters_lambda++;
+        ctl.need_jac = 1;
+        return;
+    }
+    ctl.inner++;
+    float l2 = ctl.l2base;
+    l2 = l2 * (0.5f * ctl.t);
+    if (obj < ctl.obj0 + l2) {
+        for (int j = 0; j < 3; ++j) b.lam[f * 4 + j] = b.lam_ls[f * 4 + j];
+        ctl.obj0 = obj;
+        if (ctl.iters_lambda >= c.max_iters_lambda) { ctl.active = 0; return; }
+        ctl.iters_lambda++;
+        ctl.need_jac = 1;
+    } else {
+        ctl.t = ctl.t * 0.5f;
+        if (ctl.t < 0.01f) { ctl.active = 0; return; }
+        for (int j = 0; j < 3; ++j) b.lam_ls[f * 4 + j] = b.lam[f * 4 + j] + ctl.t * b.dlam[f * 4 + j];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Neighbour maps (derivative_computer.cu:43-72; funcs.cu:81-131, 288-343), one block per
+// frame. The reference stable-sorts fragments by pixel and derives, for sorted position i,
+// left = i - (cum[p] - cum[p-256]) (0 when not positive, clamped to N-1),
+// right = i + cum[p+256] - cum[p], above/below = i -+ 1 (16-bit wrap), position 0 and N-1
+// all 0, where cum counts distinct covered pixels up to a pixel. Here the sort is replaced by
+// a counting placement: sorted position = distinct pixels below p + extra (tied) fragments
+// below p + rank among the fragments of p in slot order.
+
+__device__ __forceinline__ uint32_t cnt_at(const uint32_t *cnt, int p)
+{
+    return (cnt[p >> 1] >> ((p & 1) * 16)) & 0xFFFFu;
+}
+
+__global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
+{
+    const int f = blockIdx.x;
+    FrameCtl &ctl = b.ctl[f];
+    if (!(all_frames ? ctl.render : ctl.need_jac)) return;
+    if (threadIdx.x == 0) prof_count(b, KID_NEIGHBOURS);
+    extern __shared__ uint32_t nsm[];
+    uint32_t *cnt = nsm;                    // 32768 words: two 16-bit counts each
+    uint32_t *bits = cnt + NPIX / 2;        // 2048 words: covered pixels
+    uint32_t *tieb = bits + NPIX / 32;      // 2048 words: pixels with 2+ fragments
+    uint32_t *wU = tieb + NPIX / 32;        // 2048: distinct pixels before the word
+    uint32_t *wE = wU + NPIX / 32;          // 2048: extra fragments before the word
+    __shared__ uint32_t s_wsum[2][32];
+    __shared__ uint32_t s_flags;
+    const int tid = threadIdx.x;
+    const int N = ctl.N;
+    const Fragment *frags = b.frag + (size_t)f * NMAX;
+    int32_t *perm = b.perm + (size_t)f * NMAX;   // sorted position -> fragment
+    if (tid == 0) s_flags = 0;
+    for (int i = tid; i < NPIX / 2; i += 1024) cnt[i] = 0;
+    __syncthreads();
+    for (int n = tid; n < N; n += 1024) {
+        const int p = frags[n].pix_owner & 0xFFFF;
+        atomicAdd(&cnt[p >> 1], (p & 1) ? 0x10000u : 1u);
+    }
+    __syncthreads();
+    // per-word distinct and extra counts, then an exclusive scan over the 2048 words
+    uint32_t u2[2], e2[2];
+    for (int q = 0; q < 2; ++q) {
+        const int w = tid * 2 + q;
+        uint32_t bb = 0, tb = 0, u = 0, e = 0;
+        for (int j = 0; j < 32; ++j) {
+            const uint32_t cv = cnt_at(cnt, w * 32 + j);
+            if (cv) { bb |= 1u << j; u++; }
+            if (cv > 1) { tb |= 1u << j; e += cv - 1; }
+        }
+        bits[w] = bb; tieb[w] = tb; u2[q] = u; e2[q] = e;
+    }
+    uint32_t us = u2[0] + u2[1], es = e2[0] + e2[1];
+    uint32_t ui = us, ei = es;   // inclusive warp scans
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t a = __shfl_up_sync(0xffffffffu, ui, o), c2 = __shfl_up_sync(0xffffffffu, ei, o);
+        if (lane >= o) { ui += a; ei += c2; }
+    }
+    if (lane == 31) { s_wsum[0][warp] = ui; s_wsum[1][warp] = ei; }
+    __syncthreads();
+    if (tid < 32) {
+        uint32_t a = s_wsum[0][tid], c2 = s_wsum[1][tid];
+        uint32_t ai = a, ci = c2;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t1 = __shfl_up_sync(0xffffffffu, ai, o), t2 = __shfl_up_sync(0xffffffffu, ci, o);
+            if (tid >= o) { ai += t1; ci += t2; }
+        }
+        s_wsum[0][tid] = ai - a;
+        s_wsum[1][tid] = ci - c2;
+    }
+    __syncthreads();
+    {
+        const uint32_t ubase = s_wsum[0][warp] + ui - us, ebase = s_wsum[1][warp] + ei - es;
+        wU[tid * 2] = ubase; wE[tid * 2] = ebase;
+        wU[tid * 2 + 1] = ubase + u2[0]; wE[tid * 2 + 1] = ebase + e2[0];
+    }
+    __syncthreads();
+    auto distinct_below = [&](int p) -> uint32_t {     // covered pixels q < p
+        const int w = p >> 5, bit = p & 31;
+        return wU[w] + __popc(bits[w] & ((1u << bit) - 1u));
+    };
+    auto cum = [&](int p) -> int {                     // covered pixels q <= p
+        const int w = p >> 5, bit = p & 31;
+        return (int)(wU[w] + __popc(bits[w] & ((2u << bit) - 1u)));
+    };
+    auto sorted_pos = [&](int n) -> int {
+        const int p = frags[n].pix_owner & 0xFFFF;
+        const int w = p >> 5, bit = p & 31;
+        uint32_t pos = distinct_below(p) + wE[w];
+        uint32_t tb = tieb[w] & ((1u << bit) - 1u);
+        while (tb) {
+            const int j = __ffs(tb) - 1;
+            tb &= tb - 1;
+            pos += cnt_at(cnt, w * 32 + j) - 1;
+        }
+        if (cnt_at(cnt, p) > 1) {
+            uint32_t r = 0;
+            for (int q = 0; q < n; ++q) r += ((frags[q].pix_owner & 0xFFFF) == (uint32_t)p);
+            pos += r;
+        }
+        return (int)pos;
+    };
+    for (int n = tid; n < N; n += 1024) perm[sorted_pos(n)] = n;
+    __syncthreads();
+    int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
+    for (int n = tid; n < N; n += 1024) {
+        const int i = sorted_pos(n);
+        int S[4] = {0, 0, 0, 0};
+        if (i != 0 && i != N - 1) {
+            const int p = frags[n].pix_owner & 0xFFFF;
+            const int y = p & 255, x = p >> 8;
+            const int right = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
+            const int left = (x > 0) ? (x - 1) * DIM + y : 0;
+            const int dl = cum(p) - cum(left);
+            int kl = (i > dl) ? (i - dl) : 0;
+            kl = (uint16_t)kl;
+            if (kl >= N - 1) kl = N - 1;
+            S[0] = kl;
+            S[1] = (uint16_t)(i + cum(right) - cum(p));
+            S[2] = (uint16_t)(i - 1);
+            S[3] = (uint16_t)(i + 1);
+        }
+        for (int q = 0; q < 4; ++q) {
+            int sq = S[q];
+            if (sq >= N) { atomicOr(&s_flags, FLAG_OUT_OF_DOMAIN); sq = 0; }
+            nb[q * NMAX + n] = perm[sq];
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && s_flags) ctl.flags |= s_flags;
+}
+
+// ------------------------------------------------------------------------------------------
+// Jacobian rows dI/dtheta (newfuncs.cu:173-299, funcs.cu:224-282): one warp per fragment,
+// lanes over the expression components; pose columns after them.
+
+constexpr int JAC_WARPS = 8;
+
+__global__ void __launch_bounds__(JAC_WARPS * 32) k_jacobian(DModel m, DBatch b)
+{
+    const int f = blockIdx.y;
+    const FrameCtl &ctl = b.ctl[f];
+    if (!ctl.need_jac) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_JACOBIAN);
+    const int N = ctl.N, K = m.K, KP = m.KP, T = m.T, V = m.V;
+    const int lane = threadIdx.x & 31;
+    const float *geo = b.geo + (size_t)f * 6 * V;
+    const float *R = b.R + f * 9, *dR = b.dR + f * 27;
+    const float *tau = b.xe + (size_t)f * m.KTP + K;
+    const float phix = b.cam[f * 4], phiy = b.cam[f * 4 + 1];
+    const Fragment *frags = b.frag + (size_t)f * NMAX;
+    const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
+    const int wstride = gridDim.x * JAC_WARPS;
+    for (int n = blockIdx.x * JAC_WARPS + (threadIdx.x >> 5); n < N; n += wstride) {
+        const Fragment fr = frags[n];
+        const int tri = fr.tri;
+        const int ib = m.tl[tri], ic = m.tl[T + tri], ia = m.tl[2 * T + tri];
+        const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
+        const float b0x = geo[ib], b0y = geo[V + ib], b0z = geo[2 * V + ib];
+        const float c0x = geo[ic], c0y = geo[V + ic], c0z = geo[2 * V + ic];
+        const float a0x = geo[ia], a0y = geo[V + ia], a0z = geo[2 * V + ia];
+        const float px = (b0x * al + c0x * be) + a0x * ga;
+        const float py = (b0y * al + c0y * be) + a0y * ga;
+        const float pz = (b0z * al + c0z * be) + a0z * ga;
+        float bX, bY, bZ, cX, cY, cZ, aX, aY, aZ;
+        camera_coords(R, tau, b0x, b0y, b0z, bX, bY, bZ);
+        camera_coords(R, tau, c0x, c0y, c0z, cX, cY, cZ);
+        camera_coords(R, tau, a0x, a0y, a0z, aX, aY, aZ);
+        const float vx = (bX * al + cX * be) + aX * ga;
+        const float vy = (bY * al + cY * be) + aY * ga;
+        const float vz = (bZ * al + cZ * be) + aZ * ga;
+        const float ivz = 1.0f / vz, ivz2 = ivz * ivz;
+        const float gx = fg[n], gy = fg[NMAX + n];
+        float *row = b.J + ((size_t)f * NMAX + n) * m.KTP;
+        const float *eb = m.E + (size_t)ib * 3 * KP, *ec = m.E + (size_t)ic * 3 * KP, *ea = m.E + (size_t)ia * 3 * KP;
+        for (int k = lane; k < K; k += 32) {
+            const float tx = (eb[k] * al + ec[k] * be) + ea[k] * ga;
+            const float ty = (eb[KP + k] * al + ec[KP + k] * be) + ea[KP + k] * ga;
+            const float tz = (eb[2 * KP + k] * al + ec[2 * KP + k] * be) + ea[2 * KP + k] * ga;
+            const float REX = (tx * R[0] + ty * R[3]) + tz * R[6];
+            const float REY = (tx * R[1] + ty * R[4]) + tz * R[7];
+            const float REZ = (tx * R[2] + ty * R[5]) + tz * R[8];
+            const float nwx = (phix * ivz2) * (REX * vz - REZ * vx);
+            const float nwy = (phiy * ivz2) * (REY * vz - REZ * vy);
+            row[k] = -(gx * nwx + gy * nwy);
+        }
+        if (lane < 6) {
+            float val;
+            if (lane == 0) val = -(gx * (phix * ivz) + gy * 0.0f);
+            else if (lane == 1) val = -(gx * 0.0f + gy * (phiy * ivz));
+            else if (lane == 2) val = -(gx * (((-phix) * vx) * ivz2) + gy * (((-phiy) * vy) * ivz2));
+            else {
+                const float *d = dR + 9 * (lane - 3);
+                const float dvx = (d[0] * px + d[3] * py) + d[6] * pz;
+                const float dvy = (d[1] * px + d[4] * py) + d[7] * pz;
+                const float dvz = (d[2] * px + d[5] * py) + d[8] * pz;
+                const float dWx = (phix * ivz2) * (vz * dvx - vx * dvz);
+                const float dWy = (phiy * ivz2) * (vz * dvy - vy * dvz);
+                val = -(gx * dWx + gy * dWy);
+            }
+            row[K + lane] = val;
+        } else if (lane < 6 + (m.KTP - m.KT)) {
+            row[m.KT + lane - 6] = 0.0f;
+        }
+    }
+}
+
+// Chain rule through the normalised gradient (newfuncs.cu:417-463) of fragment n, column j.
+__device__ __forceinline__ void chain(const float *Jf, int ld, const int32_t *nb, int n, int j,
+                                      float gx, float gy, float pre, float &ox, float &oy)
+{
+    const float dh = Jf[(size_t)nb[1 * NMAX + n] * ld + j] - Jf[(size_t)nb[0 * NMAX + n] * ld + j];
+    const float dv = Jf[(size_t)nb[3 * NMAX + n] * ld + j] - Jf[(size_t)nb[2 * NMAX + n] * ld + j];
+    const float diffx = 2 * gx, diffy = 2 * gy;
+    const float X = (-diffy) * (-dh) - (-diffx) * (-dv);
+    ox = ((-pre) * (-diffy)) * X;
+    oy = (pre * (-diffx)) * X;
+}
+
+// ------------------------------------------------------------------------------------------
+// Normal equations of the image term (derivative_computer.cu:135-164), one block per frame:
+// rows of d(gx/|g|)/dtheta and d(gy/|g|)/dtheta are formed 32 fragments at a time in shared
+// memory and folded into H = tau * sum(row row^T) and g = -tau * sum(w row) with FP64
+// accumulation (4x4 register blocks of the upper triangle per thread).
+
+constexpr int NE_THREADS = 256, NE_CHUNK = 32;
+
+__global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
+{
+    const int f = blockIdx.x;
+    const FrameCtl &ctl = b.ctl[f];
+    if (!ctl.need_jac) return;
+    if (threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
+    extern __shared__ float nesm[];
+    const int KTP = m.KTP, KT = m.KT;
+    float *rows = nesm;                          // [2*NE_CHUNK][KTP]
+    float *wts = rows + 2 * NE_CHUNK * KTP;      // [2*NE_CHUNK]
+    const int tid = threadIdx.x;
+    const int nb4 = KTP / 4;
+    // upper-triangle 4x4 block owned by this thread
+    int bi = -1, bj = -1;
+    {
+        int t = tid;
+        for (int i = 0; i < nb4 && bi < 0; ++i) {
+            const int len = nb4 - i;
+            if (t < len) { bi = i; bj = i + t; } else t -= len;
+        }
+    }
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    double gacc = 0.0;
+    const int N = ctl.N;
+    const float *Jf = b.J + (size_t)f * NMAX * KTP;
+    const int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
+    const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
+    for (int n0 = 0; n0 < N; n0 += NE_CHUNK) {
+        const int cn = min(NE_CHUNK, N - n0);
+        for (int i = tid; i < NE_CHUNK * KTP; i += NE_THREADS) {
+            const int q = i / KTP, j = i - q * KTP;
+            float ox = 0.0f, oy = 0.0f;
+            if (q < cn && j < KT) {
+                const int n = n0 + q;
+                const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
+                const float pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
+                chain(Jf, KTP, nb, n, j, gx, gy, pre, ox, oy);
+            }
+            rows[(2 * q) * KTP + j] = ox;
+            rows[(2 * q + 1) * KTP + j] = oy;
+        }
+        for (int q = tid; q < NE_CHUNK; q += NE_THREADS) {
+            wts[2 * q] = q < cn ? fg[3 * NMAX + n0 + q] : 0.0f;
+            wts[2 * q + 1] = q < cn ? fg[4 * NMAX + n0 + q] : 0.0f;
+        }
+        __syncthreads();
+        if (bi >= 0) {
+            for (int q = 0; q < cn; ++q) {
+                const float4 ax = *reinterpret_cast<const float4 *>(rows + (2 * q) * KTP + 4 * bi);
+                const float4 cx = *reinterpret_cast<const float4 *>(rows + (2 * q) * KTP + 4 * bj);
+                const float4 ay = *reinterpret_cast<const float4 *>(rows + (2 * q + 1) * KTP + 4 * bi);
+                const float4 cy = *reinterpret_cast<const float4 *>(rows + (2 * q + 1) * KTP + 4 * bj);
+                const double axv[4] = {ax.x, ax.y, ax.z, ax.w}, cxv[4] = {cx.x, cx.y, cx.z, cx.w};
+                const double ayv[4] = {ay.x, ay.y, ay.z, ay.w}, cyv[4] = {cy.x, cy.y, cy.z, cy.w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] += axv[i] * cxv[j] + ayv[i] * cyv[j];
+            }
+        }
+        if (tid < KTP) {
+            for (int q = 0; q < cn; ++q)
+                gacc += (double)wts[2 * q] * (double)rows[(2 * q) * KTP + tid] +
+                        (double)wts[2 * q + 1] * (double)rows[(2 * q + 1) * KTP + tid];
+        }
+        __syncthreads();
+    }
+    const double tau = 25.0;
+    float *H = b.H + (size_t)f * KTP * KTP;
+    if (bi >= 0) {
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                const int a = 4 * bi + i, c = 4 * bj + j;
+                if (a >= KT || c >= KT) continue;
+                const float v = (float)(tau * acc[i][j]);
+                H[(size_t)a * KTP + c] = v;
+                H[(size_t)c * KTP + a] = v;
+            }
+    }
+    if (tid < KT) b.g[(size_t)f * KTP + tid] = (float)(-tau * gacc);
+}
+
+// ------------------------------------------------------------------------------------------
+// Log-barrier gradient and Gauss-Newton Hessian (logbarrier_initializer.cu:1272-1843) added
+// to the image system, one block per frame.
+
+__global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft_bounds)
+{
+    const int f = blockIdx.x;
+    const FrameCtl &ctl = b.ctl[f];
+    if (!ctl.need_jac) return;
+    if (threadIdx.x == 0) prof_count(b, KID_BARRIER);
+    extern __shared__ float bsm[];
+    const int KT = m.KT, KTP = m.KTP, K = m.K;
+    float *Fm = bsm;                              // [4*NL][KTP]
+    __shared__ float G[4][NL];
+    __shared__ float s_p[NL][3];
+    const int tid = threadIdx.x;
+    const float *x = b.x + (size_t)f * KTP;       // the accepted point (= evaluation point)
+    const float *R = b.R + f * 9, *dR = b.dR + f * 27;
+    const float *tau = x + K;
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *cam = b.cam + f * 4;
+    const float phix = cam[0], phiy = cam[1], cx = cam[2], cy = cam[3];
+    const float fs = b.face_size[f];
+    const float *bnd = b.bounds + (size_t)f * 4 * NL;
+    const float *xl = b.xl + f * NL, *yl = b.yl + f * NL;
+    if (tid < NL) {
+        const int v = m.lis[tid];
+        const float p0 = geo[v], p1 = geo[m.V + v], p2 = geo[2 * m.V + v];
+        s_p[tid][0] = p0; s_p[tid][1] = p1; s_p[tid][2] = p2;
+        const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
+        const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
+        const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
+        const float xproj = phix * ((r1p + tau[0]) / (r3p + tau[2])) + cx;
+        const float yproj = phiy * ((r2p + tau[1]) / (r3p + tau[2])) + cy;
+        G[0][tid] = 0.0f - ((xl[tid] + bnd[0 * NL + tid] * fs) - xproj);
+        G[1][tid] = 0.0f - ((yl[tid] + bnd[1 * NL + tid] * fs) - yproj);
+        G[2][tid] = 0.0f - ((xproj - bnd[2 * NL + tid] * fs) - xl[tid]);
+        G[3][tid] = 0.0f - ((yproj - bnd[3 * NL + tid] * fs) - yl[tid]);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NL * KTP; idx += 256) {
+        const int i = idx / KTP, a = idx - i * KTP;
+        const float p0 = s_p[i][0], p1 = s_p[i][1], p2 = s_p[i][2];
+        const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
+        const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
+        const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
+        const float vx = r1p + tau[0], vy = r2p + tau[1], vz = r3p + tau[2];
+        const float ivz = 1.0f / vz, ivz2 = ivz * ivz;
+        float wx = 0.0f, wy = 0.0f;
+        if (a < K) {
+            const float *ex = m.E + (size_t)m.lis[i] * 3 * m.KP;
+            const float RIX = ex[a], RIY = ex[m.KP + a], RIZ = ex[2 * m.KP + a];
+            const float dvx = (RIX * R[0] + RIY * R[3]) + RIZ * R[6];
+            const float dvy = (RIX * R[1] + RIY * R[4]) + RIZ * R[7];
+            const float dvz = (RIX * R[2] + RIY * R[5]) + RIZ * R[8];
+            wx = (phix * ivz2) * (dvx * vz - dvz * vx);
+            wy = (phiy * ivz2) * (dvy * vz - dvz * vy);
+        } else if (a < KT) {
+            const int cidx = a - K;
+            if (cidx == 0) { wx = phix * ivz; wy = 0.0f; }
+            else if (cidx == 1) { wx = 0.0f; wy = phiy * ivz; }
+            else if (cidx == 2) { wx = ((-phix) * vx) * ivz2; wy = ((-phiy) * vy) * ivz2; }
+            else {
+                const float *d = dR + 9 * (cidx - 3);
+                const float dvx = (d[0] * p0 + d[3] * p1) + d[6] * p2;
+                const float dvy = (d[1] * p0 + d[4] * p1) + d[7] * p2;
+                const float dvz = (d[2] * p0 + d[5] * p1) + d[8] * p2;
+                wx = (phix * ivz2) * (vz * dvx - vx * dvz);
+                wy = (phiy * ivz2) * (vz * dvy - vy * dvz);
+            }
+        }
+        const bool live = a < KT;
+        Fm[(0 * NL + i) * KTP + a] = live ? -wx / G[0][i] : 0.0f;
+        Fm[(1 * NL + i) * KTP + a] = live ? -wy / G[1][i] : 0.0f;
+        Fm[(2 * NL + i) * KTP + a] = live ? wx / G[2][i] : 0.0f;
+        Fm[(3 * NL + i) * KTP + a] = live ? wy / G[3][i] : 0.0f;
+    }
+    __syncthreads();
+    const float *lb = m.eps_b + (ft_bounds ? 2 : 0) * K;
+    const float *ub = m.eps_b + (ft_bounds ? 3 : 1) * K;
+    float *H = b.H + (size_t)f * KTP * KTP;
+    float *gv = b.g + (size_t)f * KTP;
+    // gradient: column sums over landmarks, set by set (the oracle's order)
+    if (tid < KT) {
+        const int a = tid;
+        double gs = 0.0;
+        for (int i = 0; i < NL; ++i)
+            for (int s = 0; s < 4; ++s) gs += (double)Fm[(s * NL + i) * KTP + a];
+        float ga = (float)gs;
+        if (a < K) {
+            const float fub = x[a] - ub[a];
+            const float flb = lb[a] - x[a];
+            ga = ga + (-1.0f / fub + 1.0f / flb);
+        }
+        gv[a] += ga;
+    }
+    // Hessian: lower triangle entries (a >= c), mirrored
+    const int npairs = KT * (KT + 1) / 2;
+    for (int pidx = tid; pidx < npairs; pidx += 256) {
+        int a = (int)((sqrtf(8.0f * (float)pidx + 1.0f) - 1.0f) * 0.5f);
+        while ((a + 1) * (a + 2) / 2 <= pidx) ++a;
+        while (a * (a + 1) / 2 > pidx) --a;
+        const int c = pidx - a * (a + 1) / 2;
+        double hs = 0.0;
+        for (int s = 0; s < 4; ++s)
+            for (int i = 0; i < NL; ++i)
+                hs += (double)Fm[(s * NL + i) * KTP + a] * (double)Fm[(s * NL + i) * KTP + c];
+        float hv = (float)hs;
+        if (a == c && a < K) {
+            const float fub = x[a] - ub[a];
+            const float flb = lb[a] - x[a];
+            const float nu = (float)(-1.0 / ((double)fub + 1e-12));
+            const float nl = (float)(1.0 / ((double)flb + 1e-12));
+            hv = hv + (nu * nu + nl * nl);
+        }
+        H[(size_t)a * KTP + c] += hv;
+        if (a != c) H[(size_t)c * KTP + a] += hv;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 Cholesky solve (solver.h:70-105) of the shape system, one block per frame, then the
+// first trial of the line search. Column j: diagonal by one thread, then the rows below in
+// parallel, each a sequential dot product over k (the oracle's order).
+
+__device__ int chol_solve_block(double *L, int n, const float *g, double *y)
+{
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_ok = 1;
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        if (tid == 0) {
+            double s = L[j * n + j];
+            for (int k = 0; k < j; ++k) s -= L[k * n + j] * L[k * n + j];
+            if (!(s > 0.0)) s_ok = 0;
+            L[j * n + j] = sqrt(s);
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        const double ljj = L[j * n + j];
+        for (int i = j + 1 + tid; i < n; i += blockDim.x) {
+            double t = L[j * n + i];
+            for (int k = 0; k < j; ++k) t -= L[k * n + i] * L[k * n + j];
+            L[j * n + i] = t / ljj;
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && s_ok) {
+        for (int i = 0; i < n; ++i) {
+            double t = (double)g[i];
+            for (int k = 0; k < i; ++k) t -= L[k * n + i] * y[k];
+            y[i] = t / L[i * n + i];
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double t = y[i];
+            for (int k = i + 1; k < n; ++k) t -= L[i * n + k] * y[k];
+            y[i] = t / L[i * n + i];
+        }
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+__global__ void __launch_bounds__(128) k_solve(DModel m, DBatch b, Cfg c, int stage)
+{
+    const int f = blockIdx.x;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.need_jac) return;
+    if (threadIdx.x == 0) prof_count(b, KID_SOLVE);
+    extern __shared__ double ssm[];
+    const int KT = m.KT, KTP = m.KTP;
+    double *L = ssm;             // [KT][KT]
+    double *y = L + KT * KT;     // [KT]
+    const float *H = b.H + (size_t)f * KTP * KTP;
+    for (int i = threadIdx.x; i < KT * KT; i += blockDim.x) {
+        const int col = i / KT, row = i - col * KT;
+        L[i] = (double)H[(size_t)col * KTP + row];
+    }
+    __syncthreads();
+    const float *gv = b.g + (size_t)f * KTP;
+    const int ok = chol_solve_block(L, KT, gv, y);
+    if (threadIdx.x != 0) return;
+    float *d = b.d + (size_t)f * KTP;
+    if (ok) { for (int i = 0; i < KT; ++i) d[i] = (float)(-y[i]); }
+    else { for (int i = 0; i < KT; ++i) d[i] = __int_as_float(0x7fc00000); ctl.flags |= FLAG_CHOL_FAILED; }
+    if (isnan(d[0])) {
+        ctl.flags |= FLAG_NAN_DIRECTION;
+        end_shape_stage(c, ctl, stage, ctl.outer);
+        return;
+    }
+    double dg = 0.0;
+    for (int a = 0; a < KT; ++a) dg += (double)d[a] * (double)gv[a];
+    ctl.l2base = (float)dg;
+    ctl.mode = M_TRIAL;
+    ctl.t = 1.0f;
+    const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
+    if (!set_trial(m, b, f, stage == ST_FINETUNE ? m.K : m.KT)) {
+        ctl.flags |= FLAG_STUCK_NEG_TZ;
+        end_shape_stage(c, ctl, stage, maxit);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Light system (derivative_computer.cu:235-312): dI/dlambda = L t (R n), chain rule, 3x3
+// normal equations in FP64, Cholesky, first trial. One block per frame.
+
+__global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
+{
+    const int f = blockIdx.x;
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.need_jac) return;
+    __shared__ double s_red[8][12];
+    __shared__ double s_L[9], s_y[3];
+    __shared__ float s_g[3];
+    const int tid = threadIdx.x, N = ctl.N;
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *R = b.R + f * 9;
+    const float *tau = b.x + (size_t)f * m.KTP + m.K;
+    const float *lam = b.lam + f * 4;
+    const float Lint = b.Lint[f];
+    const Fragment *frags = b.frag + (size_t)f * NMAX;
+    float *Jl = b.J + (size_t)f * NMAX * m.KTP;   // rows of pitch 4
+    for (int n = tid; n < N; n += 256) {
+        const Shading s = shade(m, geo, frags[n], R, tau, lam, Lint);
+        const Fragment fr = frags[n];
+        const int tri = fr.tri;
+        const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
+        const float t = (m.tex[m.tl[tri]] * al + m.tex[m.tl[m.T + tri]] * be) + m.tex[m.tl[2 * m.T + tri]] * ga;
+        const float Lt = Lint * t;
+        const float r0 = Lt * s.nn[0], r1 = Lt * s.nn[1], r2 = Lt * s.nn[2];
+        for (int j = 0; j < 3; ++j) Jl[(size_t)n * 4 + j] = (r0 * R[j] + r1 * R[j + 3]) + r2 * R[j + 6];
+        Jl[(size_t)n * 4 + 3] = 0.0f;
+    }
+    __syncthreads();
+    const int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
+    const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
+    double acc[12];
+    for (int q = 0; q < 12; ++q) acc[q] = 0.0;
+    for (int n = tid; n < N; n += 256) {
+        const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
+        const float pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
+        float ox[3], oy[3];
+        for (int j = 0; j < 3; ++j) chain(Jl, 4, nb, n, j, gx, gy, pre, ox[j], oy[j]);
+        const double sx = fg[3 * NMAX + n], sy = fg[4 * NMAX + n];
+        for (int a = 0; a < 3; ++a) {
+            acc[9 + a] += sx * ox[a] + sy * oy[a];
+            for (int bb = 0; bb < 3; ++bb) acc[a * 3 + bb] += (double)ox[a] * ox[bb] + (double)oy[a] * oy[bb];
+        }
+    }
+    for (int q = 0; q < 12; ++q)
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+    if ((tid & 31) == 0)
+        for (int q = 0; q < 12; ++q) s_red[tid >> 5][q] = acc[q];
+    __syncthreads();
+    if (tid != 0) return;
+    double tot[12];
+    for (int q = 0; q < 12; ++q) { tot[q] = 0.0; for (int w = 0; w < 8; ++w) tot[q] += s_red[w][q]; }
+    float Hf[9];
+    for (int i = 0; i < 9; ++i) Hf[i] = (float)tot[i];
+    for (int i = 0; i < 3; ++i) s_g[i] = (float)(-tot[9 + i]);
+    // 3x3 Cholesky in the oracle's order (single thread)
+    int ok = 1;
+    for (int i = 0; i < 9; ++i) s_L[i] = (double)Hf[i];
+    for (int j = 0; j < 3 && ok; ++j) {
+        double s = s_L[j * 3 + j];
+        for (int k = 0; k < j; ++k) s -= s_L[k * 3 + j] * s_L[k * 3 + j];
+        if (!(s > 0.0)) { ok = 0; break; }
+        const double ljj = sqrt(s);
+        s_L[j * 3 + j] = ljj;
+        for (int i = j + 1; i < 3; ++i) {
+            double t = s_L[j * 3 + i];
+            for (int k = 0; k < j; ++k) t -= s_L[k * 3 + i] * s_L[k * 3 + j];
+            s_L[j * 3 + i] = t / ljj;
+        }
+    }
+    float dl[3];
+    if (ok) {
+        for (int i = 0; i < 3; ++i) {
+            double t = (double)s_g[i];
+            for (int k = 0; k < i; ++k) t -= s_L[k * 3 + i] * s_y[k];
+            s_y[i] = t / s_L[i * 3 + i];
+        }
+        for (int i = 2; i >= 0; --i) {
+            double t = s_y[i];
+            for (int k = i + 1; k < 3; ++k) t -= s_L[i * 3 + k] * s_y[k];
+            s_y[i] = t / s_L[i * 3 + i];
+        }
+        for (int i = 0; i < 3; ++i) dl[i] = (float)(-s_y[i]);
+    } else {
+        for (int i = 0; i < 3; ++i) dl[i] = __int_as_float(0x7fc00000);
+    }
+    for (int j = 0; j < 3; ++j) { b.dlam[f * 4 + j] = dl[j]; b.glam[f * 4 + j] = s_g[j]; }
+    const float l2 = (float)((double)dl[0] * s_g[0] + (double)dl[1] * s_g[1] + (double)dl[2] * s_g[2]);
+    ctl.l2base = l2;
+    ctl.mode = M_TRIAL;
+    ctl.t = 1.0f;
+    for (int j = 0; j < 3; ++j) b.lam_ls[f * 4 + j] = lam[j] + 1.0f * dl[j];
+    // the first trial's -g.d test (model_fitter.cu:1044-1048) does not depend on the trial
+    if ((double)(-l2) < 0.0003 || !(l2 == l2)) ctl.active = 0;
+}
+
+// Unblurred image and owner-triangle map of every rendering frame (renderer.cu:635-696).
+__global__ void k_paint(DModel m, DBatch b, float *images, int32_t *tri_map)
+{
+    const int f = blockIdx.y;
+    const FrameCtl &ctl = b.ctl[f];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < NPIX; p += gridDim.x * blockDim.x) {
+        images[(size_t)f * NPIX + p] = 0.0f;
+        tri_map[(size_t)f * NPIX + p] = -1;
+    }
+    if (!ctl.render) return;
+    __syncthreads();
+    // the clear above and the writes below touch disjoint work of one frame only when the
+    // grid has a single block in x; the host launches it that way
+    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float *R = b.R + f * 9;
+    const float *tau = b.xe + (size_t)f * m.KTP + m.K;
+    const float *lam = b.lam + f * 4;
+    const Fragment *frags = b.frag + (size_t)f * NMAX;
+    for (int n = threadIdx.x; n < ctl.N; n += blockDim.x) {
+        const Fragment fr = frags[n];
+        if (!(fr.pix_owner & 0x80000000u)) continue;
+        const Shading s = shade(m, geo, fr, R, tau, lam, b.Lint[f]);
+        const int p = fr.pix_owner & 0xFFFF;
+        images[(size_t)f * NPIX + p] = s.tex;
+        tri_map[(size_t)f * NPIX + p] = fr.tri;
+    }
+}
+
+// Frames still running the current stage.
+__global__ void k_count_active(DBatch b, int *out)
+{
+    __shared__ int s;
+    if (threadIdx.x == 0) s = 0;
+    __syncthreads();
+    int c = 0;
+    for (int f = threadIdx.x; f < b.F; f += blockDim.x) c += b.ctl[f].active;
+    atomicAdd(&s, c);
+    __syncthreads();
+    if (threadIdx.x == 0) *out = s;
+}
+
+}  // namespace tdi

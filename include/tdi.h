@@ -1,0 +1,177 @@
+/*
+ * tdi.h -- C ABI of the B200 implementation of 3DI's per-frame 3DMM fitting path.
+ *
+ * The path replaced is VideoFitter::fit_to_video_frame after the landmark initialisation
+ * (src/lib/video_fitter.cu:432-648 of Computational-Psychiatry/3DI): blur of the target
+ * crop, the light fit fit_3DMM_lambdas (src/lib/model_fitter.cu:981-1073), the shape fit
+ * fit_3DMM_shape_rigid (model_fitter.cu:121-375), the optional two-stage repetition and
+ * the expression finetune fit_3DMM_epsilon_finetune (model_fitter.cu:397-672), with the
+ * renderer, derivative and solver calls they make (src/lib/renderer.cu,
+ * derivative_computer.cu, logbarrier_initializer.cu, solver.h).
+ *
+ * Conventions: plain pointers and sizes, no CUDA or torch types (a stream is passed as
+ * void*, NULL = the default stream); no global state; the caller owns inputs and outputs,
+ * the library owns device scratch; errors are status codes (tdi_last_error() gives a
+ * message). Images are 256x256 float crops stored column-major (pixel (x, y) at x*256+y),
+ * as the reference stores them (video_fitter.cu:543-546).
+ */
+#ifndef TDI_H
+#define TDI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t tdi_status;
+#define TDI_OK 0
+#define TDI_ERR_INVALID 1       /* bad argument */
+#define TDI_ERR_CUDA 2          /* a CUDA call failed */
+#define TDI_ERR_NOMEM 3         /* device or host allocation failed */
+#define TDI_ERR_CAPACITY 4      /* more frames than the batch holds */
+
+/* per-frame status bits of tdi_report.flags */
+#define TDI_FLAG_RENDER_SKIPPED 1u   /* visible fragments outside [1000, 52000]: the reference
+                                        skips the render (renderer.cu:669-677); frame stops */
+#define TDI_FLAG_OUT_OF_DOMAIN 2u    /* an input the reference leaves undefined (fragments
+                                        outside the crop or on its border, > 25,600 fragments) */
+#define TDI_FLAG_NAN_DIRECTION 4u    /* NaN search direction (model_fitter.cu:206-213) */
+#define TDI_FLAG_STUCK_NEG_TZ 8u     /* a trial with tau_z < 0 (model_fitter.cu:255-259) */
+#define TDI_FLAG_CHOL_FAILED 16u     /* Cholesky factorisation failed (solver.h:87-92) */
+#define TDI_FLAG_FAIL 32u            /* outer iterations <= NITERS_SUCCESS (model_fitter.cu:374) */
+#define TDI_FLAG_OVERFLOW 64u        /* more than 32,768 fragments */
+
+typedef struct tdi_model tdi_model;
+typedef struct tdi_batch tdi_batch;
+
+/* Morphable model with the subject's identity applied (replaces the Renderer constructor's
+ * file loading, renderer.cu:22-442, and the identity files of video_from_saved_identity.cu:
+ * 141-150). Host arrays, copied to the device. */
+typedef struct {
+    int32_t n_vertices;          /* V */
+    int32_t n_triangles;         /* T (the reference's 16-bit indices cap T at 65,535) */
+    int32_t n_expr;              /* K, 79 for the GLOBAL79 basis */
+    const float *mean;           /* [3][V] X0_mean, Y0_mean, Z0_mean (identity applied) */
+    const float *expr_basis;     /* [V][3][K] rows of EX_79/EY_79/EZ_79.dat per vertex */
+    const float *tex;            /* [V] albedo (tex_mu with the identity texture) */
+    const int32_t *triangles;    /* [3][T] 0-based vertex ids (tl.dat columns minus 1) */
+    const int32_t *landmarks;    /* [51] landmark vertex ids (config::LIS) */
+    const float *eps_lb;         /* [K] expression bounds of the shape fit */
+    const float *eps_ub;
+    const float *eps_lb_finetune;/* [K] bounds of the expression finetune */
+    const float *eps_ub_finetune;
+} tdi_model_desc;
+
+/* Frames of a batch; host arrays. The crop origin and face size follow the reference
+ * (renderer.cu:580-598, funcs.cu:44-54) when x0y0 is NULL or face_size is NULL. */
+typedef struct {
+    int32_t n_frames;            /* F */
+    const float *targets;        /* [F][65536] unblurred gray crops (the library blurs them) */
+    const float *xl, *yl;        /* [F][51] landmarks in the rescaled frame */
+    const float *bounds;         /* [F][4][51] lx, ly, ux, uy bound offsets in face sizes */
+    const float *face_size;      /* [F] or NULL */
+    const float *cam;            /* [F][4] phix, phiy, cx, cy of the rescaled camera */
+    const int32_t *x0y0;         /* [F][2] crop origins, or NULL */
+} tdi_frames;
+
+/* Configuration keys of the reference that the path reads (config.cu:350-541). */
+typedef struct {
+    int32_t max_iters_rigid;     /* outer GN iterations of the shape fit (100) */
+    int32_t max_iters_finetune;  /* outer GN iterations of the finetune (100) */
+    int32_t twostage_illum;      /* TWOSTAGE_ILLUM */
+    int32_t finetune;            /* FINETUNE_EXPRESSIONS */
+    int32_t niters_success;      /* NITERS_SUCCESS (6) */
+    int32_t max_iters_lambda;    /* outer iterations of the light fit (10000) */
+    float ref_face_size;         /* REF_FACE_SIZE */
+    float taps[15];              /* Gaussian taps for KERNEL_SIGMA (video_fitter.cu:53-61) */
+} tdi_fit_config;
+
+typedef struct {
+    uint32_t flags;              /* TDI_FLAG_* */
+    int32_t n_fragments;         /* visible fragments of the last render */
+    int32_t iters_rigid;         /* num_outer_iters summed over the shape fits */
+    int32_t iters_finetune;
+    int32_t iters_lambda;        /* outer light-fit iterations */
+    int32_t renders;             /* rasterisations */
+    float objective;             /* last accepted objective */
+} tdi_report;
+
+const char *tdi_last_error(void);
+
+/* Model: replaces the Renderer/Logbarrier_Initializer model loading
+ * (renderer.cu:22-442, logbarrier_initializer.cu:30-440). */
+tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out);
+tdi_status tdi_model_destroy(tdi_model *m);
+
+/* Batch: device working set for up to max_frames frames fitted together (replaces the
+ * per-VideoFitter Optimizer/OptimizationVariables/Solver allocations, Optimizer.h:24-361). */
+tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out);
+tdi_status tdi_batch_destroy(tdi_batch *b);
+
+/* Upload frames and blur the targets (video_fitter.cu:537-550). Synchronous. */
+tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *frames, void *stream);
+/* Upload states: x [F][K+6] (epsilon, tau_x, tau_y, tau_z, u1, u2, u3), lam [F][3],
+ * light intensity L [F]. Synchronous. */
+tdi_status tdi_batch_set_state(tdi_batch *b, const float *x, const float *lam, const float *L,
+                               void *stream);
+/* Fit every frame of the batch on the device (asynchronous on the stream apart from one
+ * 4-byte read-back per round). Replaces fit_to_video_frame's fitting calls. */
+tdi_status tdi_batch_fit(tdi_batch *b, const tdi_fit_config *cfg, void *stream);
+/* Download states and reports. Synchronous. */
+tdi_status tdi_batch_get_state(tdi_batch *b, float *x, float *lam, tdi_report *rep, void *stream);
+
+/* All of the above for host buffers: upload, fit, download (x and lam are in/out). */
+tdi_status tdi_fit_frames(tdi_batch *b, const tdi_frames *frames, const tdi_fit_config *cfg,
+                          float *x, float *lam, const float *L, tdi_report *rep, void *stream);
+
+/* One full evaluation of every frame at its current state -- what one outer iteration of
+ * fit_3DMM_shape_rigid computes before its line search (get_obj_hessian_and_gradient_multiframe
+ * and Solver::solve, model_fitter.cu:21-116,179-201) -- kept on the device for
+ * tdi_batch_read. finetune_bounds selects the finetune expression bounds. */
+tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t finetune_bounds,
+                              void *stream);
+
+/* Read one frame's working set after tdi_batch_evaluate or tdi_batch_raster. what:
+ *  0 fragments   int32 [N][4]: pixel | owner<<31, triangle, float bits of alpha, beta
+ *  1 neighbours  int32 [4][N]: kl, kr, ka, kb
+ *  2 gradients   float [5][N]: gx, gy, h, target gx/|g|, target gy/|g|
+ *  3 jacobian    float [N][K+6]
+ *  4 normal eq.  float [K+6][K+6] H, then [K+6] g, then [K+6] direction d
+ *  5 scalars     double [4]: correlation, barrier objective, objective, face check
+ *  6 geometry    float [6][V]: X0, Y0, Z0, xp, yp, camera Z
+ * Returns the number of elements written through *count. Synchronous. */
+tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, int64_t capacity,
+                          int64_t *count);
+
+/* Visibility of given projections (the reference's get_pixels_to_render, keep_only_minZ and
+ * remove_if, funcs.cu:900-1029, renderer.cu:650-680) for one frame slot of the batch: xp, yp
+ * and camera Z per vertex, crop origin. Results are read with tdi_batch_read(what=0).
+ * Synchronous; returns the fragment count through *n_out. */
+tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const float *yp,
+                            const float *zc, int32_t x0, int32_t y0, int32_t *n_out,
+                            uint32_t *flags_out);
+
+/* Render every frame of the batch at its current state, as Renderer::render does before
+ * the blur (renderer.cu:635-696): unblurred image [F][65536] and the triangle that owns each
+ * pixel [F][65536] (-1 where nothing is drawn). Either output may be NULL. Synchronous. */
+tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void *stream);
+
+/* Kernels launched by this batch since it was created (each a hand-written CUDA kernel). */
+tdi_status tdi_batch_launches(tdi_batch *b, int64_t *launches);
+
+/* Live timing of one kernel for roofline reports: while kernel_id != 0, every launch of that
+ * kernel is bracketed by CUDA events on its stream and the frames it processed are counted
+ * on the device. kernel_id: 1 vertex stage, 2 visibility, 3 render, 4 neighbour maps,
+ * 5 Jacobian rows, 6 normal equations, 7 barrier terms, 8 Cholesky. profile_read returns the
+ * launches, their summed milliseconds and the frames they processed since profile() was
+ * called (synchronises). */
+tdi_status tdi_batch_profile(tdi_batch *b, int32_t kernel_id);
+tdi_status tdi_batch_profile_read(tdi_batch *b, int64_t *launches, double *total_ms,
+                                  int64_t *frames);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDI_H */

@@ -1,0 +1,119 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle on the same seeded inputs.
+
+Bit-exact: vertex stage, visibility (fragment list in slot order, pixel owners), neighbour
+maps, image gradients and Jacobian rows. Within tolerance: the normal equations (FP64 sums in
+a different order; tolerance 1e-6 relative), the search direction (1e-4 relative to its norm)
+and fitted states (1e-5 relative parameter error)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(tdi, case, synth):
+    tdi.require_gpu()
+    m, fr, om = case
+    model = tdi.Model(m)
+    batch = tdi.Batch(model, fr.n_frames)
+    batch.set_frames(fr)
+    lam = np.tile(synth.LAMBDA_INIT, (fr.n_frames, 1))
+    L = np.full(fr.n_frames, synth.L_INTENSITY, np.float32)
+    return model, batch, lam, L
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+def test_raster_bit_exact_on_same_projections(request, tdi, synth, O, case_name):
+    case = request.getfixturevalue(case_name)
+    m, fr, om = case
+    model, batch, lam, L = _setup(tdi, case, synth)
+    for i in range(fr.n_frames):
+        for state in (fr.state_true[i], fr.state_init[i]):
+            geo, ok = O.vertex_stage(om, state, fr.cam[i])
+            xp, yp, Z = geo[6], geo[7], geo[5]
+            x0, y0 = (int(v) for v in fr.x0y0[i])
+            ref = O.raster(om, xp, yp, Z, x0, y0)
+            n, flags = batch.raster(i, xp, yp, Z, x0, y0)
+            got = batch.read(i, tdi.READ_FRAGMENTS)
+            assert n == ref["N"]
+            assert np.array_equal(got["pix"], ref["pix"])
+            assert np.array_equal(got["tri"], ref["tri"])
+            assert np.array_equal(_bits(got["al"]), _bits(ref["al"]))
+            assert np.array_equal(_bits(got["be"]), _bits(ref["be"]))
+            assert np.array_equal(got["owner"], ref["owner"])
+
+
+@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+def test_evaluate_matches_oracle(request, tdi, synth, O, case_name):
+    case = request.getfixturevalue(case_name)
+    m, fr, om = case
+    model, batch, lam, L = _setup(tdi, case, synth)
+    cfg = tdi.default_config()
+    ocfg = O.config()
+    fs = O.FrameSet(fr)
+    batch.set_state(fr.state_init, lam, L)
+    batch.evaluate(cfg)
+    K = m.n_expr
+    for i in range(fr.n_frames):
+        e = O.evaluate(om, fs, i, ocfg, fr.state_init[i], lam[i], float(L[i]))
+        geo = batch.read(i, tdi.READ_GEOMETRY)
+        ogeo, _ = O.vertex_stage(om, fr.state_init[i], fr.cam[i])
+        for gi, oi in ((0, 0), (1, 1), (2, 2), (3, 6), (4, 7), (5, 5)):
+            assert np.array_equal(_bits(geo[gi]), _bits(ogeo[oi])), ("geometry", gi)
+        fr_g = batch.read(i, tdi.READ_FRAGMENTS)
+        assert len(fr_g["pix"]) == e["N"]
+        assert np.array_equal(fr_g["pix"], e["pix"]) and np.array_equal(fr_g["tri"], e["tri"])
+        assert np.array_equal(fr_g["owner"], e["owner"])
+        nb = batch.read(i, tdi.READ_NEIGHBOURS)
+        assert np.array_equal(nb, e["nb"])
+        gr = batch.read(i, tdi.READ_GRADIENTS)
+        og = e["grads"]
+        for gi, oi in ((0, 0), (1, 1), (2, 2), (3, 5), (4, 6)):
+            assert np.array_equal(_bits(gr[gi]), _bits(og[oi])), ("gradient", gi)
+        J = batch.read(i, tdi.READ_JACOBIAN)
+        assert np.array_equal(_bits(J), _bits(e["J"]))
+        ne = batch.read(i, tdi.READ_NORMAL_EQ)
+        scale = np.abs(e["H"]).max()
+        np.testing.assert_allclose(ne["H"], e["H"], rtol=1e-6, atol=1e-6 * scale)
+        np.testing.assert_allclose(ne["g"], e["g"], rtol=1e-6, atol=1e-6 * np.abs(e["g"]).max())
+        dn = np.linalg.norm(e["d"])
+        assert np.linalg.norm(ne["d"] - e["d"]) <= 1e-4 * dn
+        sc = batch.read(i, tdi.READ_SCALARS)
+        assert abs(sc["corr"] - e["corr"]) <= 1e-9 * abs(e["corr"])
+        assert abs(sc["barrier"] - e["barrier"]) <= 1e-6 * abs(e["barrier"])
+        assert abs(sc["objective"] - e["objective"]) <= 1e-6 * abs(e["objective"])
+        assert sc["face_ok"] == e["face_ok"]
+
+
+def test_fit_matches_oracle(tdi, synth, O, small_case):
+    m, fr, om = small_case
+    model, batch, lam, L = _setup(tdi, small_case, synth)
+    cfg = tdi.default_config(max_iters_rigid=10)
+    x, lamf, rep = batch.fit_frames(fr, fr.state_init, lam, L, cfg)
+    ox, olam, orep = O.fit_frames(om, O.FrameSet(fr), O.config(max_iters_rigid=10), fr.state_init, lam, L)
+    for i in range(fr.n_frames):
+        assert rep[i].flags == orep[i].flags
+        assert rep[i].iters_rigid == orep[i].iters_rigid
+        assert rep[i].iters_lambda == orep[i].iters_lambda
+        assert rep[i].n_fragments == orep[i].n_fragments
+        err = np.abs(x[i] - ox[i]) / np.maximum(np.abs(ox[i]), 1e-2)
+        assert err.max() <= 1e-5, err.max()
+        np.testing.assert_allclose(lamf[i], olam[i], rtol=1e-5, atol=1e-7)
+
+
+def test_render_skipped_frame_is_flagged_and_left_unchanged(tdi, synth, O, small_case):
+    """A face too small to give 1,000 fragments: the reference skips the render
+    (renderer.cu:669-677); the frame is flagged and its state stays where it started."""
+    m, fr, om = small_case
+    model, batch, lam, L = _setup(tdi, small_case, synth)
+    x = fr.state_init.copy()
+    x[0, m.n_expr + 2] *= 4.0          # four times farther away: a quarter of the size
+    cfg = tdi.default_config(max_iters_rigid=5)
+    xo, lamo, rep = batch.fit_frames(fr, x, lam, L, cfg)
+    assert rep[0].flags & tdi.FLAG_RENDER_SKIPPED
+    assert rep[0].flags & tdi.FLAG_FAIL
+    assert np.array_equal(xo[0], x[0])
+    assert not rep[1].flags & tdi.FLAG_RENDER_SKIPPED
