@@ -343,9 +343,9 @@ __device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, c
         xlo_f = xlo_f >= 0.0f ? xlo_f : 0.0f;
         ylo_f = ylo_f >= 0.0f ? ylo_f : 0.0f;
     }
-    // A triangle whose box spans millions of pixels only arises from a vertex near the camera
+    // A triangle whose box exceeds the whole crop only arises from a vertex near the camera
     // plane; the reference would walk the whole box. It is skipped and flagged instead.
-    if ((xhi - xlo_f) * (yhi - ylo_f) > 4194304.0f) {
+    if ((xhi - xlo_f) * (yhi - ylo_f) > 65536.0f) {
         flags |= FLAG_OUT_OF_DOMAIN;
         return 0;
     }

@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Throughput of the batched 3DMM video fit (fitted frames/s) on B200.
+
+Workload "cap53k_video": the seeded synthetic morphable model with the shapes of the
+reference's full-size model (53,490 vertices, 106,466 triangles, 79 expression components),
+a batch of video frames (AR(1) expressions, random-walk head pose, face boxes 120-600 px in
+1080p) rescaled to the reference's 256x256 crop, fitted per frame as
+VideoFitter::fit_to_video_frame does after its landmark initialisation: light fit, then the
+log-barrier Gauss-Newton shape fit (pose + 79 expressions) capped at 20 outer iterations.
+
+One step = one fit of the whole batch. ``value`` times ``tdi_batch_fit`` with every input
+resident in device memory; ``e2e`` times ``tdi_fit_frames`` from pinned host buffers
+(host->device copy of the frames and states, the fit, and the read-back of states and reports).
+Inputs (256 MB of target crops for 1,024 frames) exceed the 126 MB L2 between steps.
+
+``--impl reference`` times the CPU restatement of the same path (oracle/, OpenMP over frames,
+all host threads) on a bounded sample of the same frames: 3DI cannot be built here (it needs
+OpenCV) and has no CPU path of its own.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "cap53k_video"
+MAX_ITERS = 20
+METRIC = "fitted frames/s (batched video fit, 53,490-vertex model, 256x256 crop)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=1024, help="frames per GPU per step")
+    ap.add_argument("--cpu-frames", type=int, default=8, help="frames of the CPU sample")
+    ap.add_argument("--profile-kernel", default="raster")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_workload(synth, n_frames, seed_offset=0):
+    spec = synth.WORKLOADS[WORKLOAD]
+    m = synth.make_model(spec["n_vertices"], spec["n_triangles"], spec["config_id"])
+    fr = synth.make_frames(m, n_frames, spec["config_id"] + seed_offset, **spec["frames"])
+    return m, fr
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), p.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def algorithmic_bytes_per_frame(kernel: str, V: int, T: int, K: int, n_frag: float) -> float:
+    """Bytes a kernel must move per frame it processes (what the roofline divides by)."""
+    if kernel == "raster":
+        # projected vertices (xp, yp, Z) + triangle indices + the fragment list written
+        return 3 * V * 4 + 3 * T * 4 + n_frag * 16
+    if kernel == "vertex":
+        # output planes per frame; the basis (3*V*K*4) is shared across the launch's frames
+        return 6 * V * 4 + K * 4
+    if kernel == "render":
+        # fragments, three vertices' object coordinates and albedo, four target pixels, gradients
+        return n_frag * (16 + 3 * 16 + 4 * 4 + 5 * 4)
+    if kernel == "jacobian":
+        # three vertices' basis rows (3 coords x K) and the row written
+        return n_frag * (3 * 3 * K * 4 + (K + 6) * 4)
+    raise ValueError(kernel)
+
+
+def cpu_fit_rate(O, synth, m, fr, n_frames, threads):
+    """Frames/s of the oracle (FP32 restatement) on the first n_frames frames."""
+    om = O.Model(m)
+    fs = O.FrameSet(fr, 0, n_frames)
+    cfg = O.config(max_iters_rigid=MAX_ITERS)
+    lam = np.tile(synth.LAMBDA_INIT, (n_frames, 1))
+    L = np.full(n_frames, synth.L_INTENSITY, np.float32)
+    t0 = time.perf_counter()
+    O.fit_frames(om, fs, cfg, fr.state_init[:n_frames], lam, L, threads=threads)
+    return n_frames / (time.perf_counter() - t0)
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    synth = importlib.import_module("3di_b200.synth")
+    O.build()
+    n = args.cpu_frames
+    m, fr = make_workload(synth, n)
+    render_targets_cpu(O, synth, m, fr)
+    threads = O.max_threads()
+    rates = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_fit_rate(O, synth, m, fr, n, threads)
+    for _ in range(args.steps):
+        rates.append(cpu_fit_rate(O, synth, m, fr, n, threads))
+    v = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "frames_per_step": n, "max_outer_iters": MAX_ITERS,
+                   "l2": "inputs larger than L2 are not applicable on the CPU"},
+        "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} frames of {WORKLOAD}, FP32 CPU restatement (oracle/), "
+                                   "3DI itself needs OpenCV and cannot be built"},
+        "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def render_targets_cpu(O, synth, m, fr):
+    om = O.Model(m)
+    cfg = O.config()
+    imgs = [O.render_target(om, fr, i, cfg, fr.state_true[i], fr.lam_true[i], synth.L_INTENSITY)[0]
+            for i in range(fr.n_frames)]
+    fr.target = synth.add_noise(np.stack(imgs), 0.02, 3)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    tdi = importlib.import_module("3di_b200")
+    synth = importlib.import_module("3di_b200.synth")
+    tdi.require_gpu()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+
+    F = args.frames
+    m, fr = make_workload(synth, F, seed_offset=100 * rank)
+    model = tdi.Model(m)
+    batch = tdi.Batch(model, F)
+    # synthetic photos: the library renders the true states, noise is added on the host
+    lam_true = fr.lam_true
+    L = np.full(F, synth.L_INTENSITY, np.float32)
+    fr.target = np.zeros((F, tdi.NPIX), np.float32)
+    batch.set_frames(fr)
+    batch.set_state(fr.state_true, lam_true, L)
+    img, _ = batch.render()
+    fr.target = synth.add_noise(img, 0.02, 3 + rank)
+    batch.set_frames(fr)
+    lam0 = np.tile(synth.LAMBDA_INIT, (F, 1)).astype(np.float32)
+    cfg = tdi.default_config(max_iters_rigid=MAX_ITERS)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        batch.set_state(fr.state_init, lam0, L)
+        batch.fit(cfg)
+    torch.cuda.synchronize()
+
+    # timed: device-resident inputs
+    clocks = ClockSampler(local)
+    clocks.start()
+    batch.profile(args.profile_kernel)
+    launches0 = batch.launches()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        batch.set_state(fr.state_init, lam0, L)      # reset the fitted states (not timed)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.fit(cfg)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        total_ms += e0.elapsed_time(e1)
+    launches = batch.launches() - launches0
+    prof_launches, prof_ms, prof_frames = batch.profile_read()
+    batch.profile(None)
+    clk = clocks.stop()
+    x, lamf, rep = batch.get_state()
+    n_frag = float(np.mean([r.n_fragments for r in rep]))
+
+    # timed: end to end from pinned host memory through tdi_fit_frames
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    h = dict(t=pin(fr.target.astype(np.float32)), xl=pin(fr.xl), yl=pin(fr.yl), b=pin(fr.bounds),
+             fs=pin(fr.face_size), cam=pin(fr.cam), o=pin(fr.x0y0.astype(np.int32)),
+             x=pin(fr.state_init), lam=pin(lam0), L=pin(L))
+    desc = tdi.FramesDesc(F, *[h[k].data_ptr() for k in ("t", "xl", "yl", "b", "fs", "cam", "o")])
+    reps = (tdi.Report * F)()
+    lib = tdi.load_library()
+    import ctypes as C
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        xs = h["x"].clone().pin_memory()
+        ls = h["lam"].clone().pin_memory()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = lib.tdi_fit_frames(batch.handle, C.byref(desc), C.byref(cfg), C.c_void_p(xs.data_ptr()),
+                                C.c_void_p(ls.data_ptr()), C.c_void_p(h["L"].data_ptr()), reps, None)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        if st != 0:
+            raise tdi.TdiError(lib.tdi_last_error().decode())
+        e2e_ms += e0.elapsed_time(e1)
+    h2d = sum(h[k].numel() * h[k].element_size() for k in ("t", "xl", "yl", "b", "fs", "cam", "o", "x", "lam", "L"))
+    d2h = F * (m.n_expr + 6) * 4 + F * 3 * 4 + F * C.sizeof(tdi.Report)
+
+    # max over ranks
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = t.tolist()
+    frames_all = F * world * args.steps
+    value = frames_all / (total_ms / 1000.0)
+    e2e = frames_all / (e2e_ms / 1000.0)
+
+    hbm, tfl, peak_kind = measured_peaks()
+    per_frame = algorithmic_bytes_per_frame(args.profile_kernel, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
+    avg_launch_s = prof_ms / 1000.0 / max(prof_launches, 1)
+    frames_per_launch = prof_frames / max(prof_launches, 1)
+    achieved = per_frame * frames_per_launch / avg_launch_s / 1e9 if prof_launches else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f).get(args.profile_kernel)
+        if tr:
+            traffic = tr["dram_bytes_per_frame"] * frames_per_launch
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded morphable model and frames)",
+        "config": {"workload": WORKLOAD, "frames_per_gpu_per_step": F,
+                   "vertices": m.n_vertices, "triangles": m.n_triangles, "expr": m.n_expr,
+                   "max_outer_iters": MAX_ITERS, "crop": "256x256",
+                   "mean_fragments": n_frag,
+                   "l2": "inputs larger than L2 (256 MB of crops per 1,024 frames)",
+                   "parallelism": f"frames sharded over {world} GPU(s), no collective"},
+        "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": args.profile_kernel, "bound": "hbm", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "launches": prof_launches,
+                     "avg_launch_ms": avg_launch_s * 1000.0, "frames_per_launch": frames_per_launch,
+                     "algorithmic_bytes_per_frame": per_frame},
+        "clocks": clk,
+        "fit": {"mean_iters_rigid": float(np.mean([r.iters_rigid for r in rep])),
+                "mean_iters_lambda": float(np.mean([r.iters_lambda for r in rep])),
+                "mean_renders": float(np.mean([r.renders for r in rep])),
+                "failed": int(sum(1 for r in rep if r.flags & tdi.FLAG_FAIL))},
+    }
+    if rank == 0 and world == 1:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.build()
+        n = min(args.cpu_frames, F)
+        threads = O.max_threads()
+        rate = cpu_fit_rate(O, synth, m, fr, n, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "frames/s", "cores": threads, "kind": "port",
+                                "sample": f"first {n} frames of the same batch, FP32 CPU restatement"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    model.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -192,9 +192,9 @@ int o_raster(const o_model *m, const float *xp, const float *yp, const float *Zc
         const uint16_t xlo = to_u16_floor(fminf(fminf(bx, cx), ax), flags);
         const uint16_t ylo = to_u16_floor(fminf(fminf(by, cy), ay), flags);
         if (!(xhi <= 65535.0f && yhi <= 65535.0f)) { *flags |= O_FLAG_OUT_OF_DOMAIN; cnt[idx] = 0; continue; }
-        /* a box of millions of pixels only comes from a vertex near the camera plane; the
+        /* a box larger than the crop only comes from a vertex near the camera plane; the
            reference would walk all of it -- skipped and flagged */
-        if ((xhi - (float)xlo) * (yhi - (float)ylo) > 4194304.0f) { *flags |= O_FLAG_OUT_OF_DOMAIN; cnt[idx] = 0; continue; }
+        if ((xhi - (float)xlo) * (yhi - (float)ylo) > 65536.0f) { *flags |= O_FLAG_OUT_OF_DOMAIN; cnt[idx] = 0; continue; }
         int ridx = 0;
         for (uint16_t x = xlo; (float)x < xhi && ridx < NTMP; ++x) {
             for (uint16_t y = ylo; (float)y < yhi && ridx < NTMP; ++y) {
@@ -937,10 +937,13 @@ static int fit_shape(ctx_t *c, real *x, real *x_ls, const real *lam, real Lint, 
                 c->rep->flags |= O_FLAG_STUCK_NEG_TZ;
                 terminate = 1; num_outer = max_iters; break;
             }
-            int face_ok = geometry_and_raster(c, x_ls, 0);
+            int face_ok = geometry(c, x_ls, 0);
             if (!face_ok) { t = t * BETA; continue; }
             double obi = barrier(m, c->f, x_ls, c->R, NULL, finetune, NULL, NULL);
             if (isnan(obi)) { t = t * BETA; continue; }
+            /* the -g.d test (model_fitter.cu:338-342) does not depend on the trial's render */
+            if ((double)(-l2base) < 0.0003) { terminate = 1; break; }
+            raster_frame(c);
             if (c->rep->flags & O_FLAG_RENDER_SKIPPED) { terminate = 2; break; }
             double corr_t = image_term(c, x_ls, lam, Lint);
             real gc = tau_img * (real)corr_t;
@@ -948,7 +951,6 @@ static int fit_shape(ctx_t *c, real *x, real *x_ls, const real *lam, real Lint, 
             real obj_tmp = -gc;
             inner++;
             real l2 = l2base;
-            if ((double)(-l2) < 0.0003) { terminate = 1; break; }
             l2 = l2 * (ALPHA * t);
             if (obj_tmp < obj + l2) {
                 for (int a = 0; a < KT; ++a) x[a] = x_ls[a];
