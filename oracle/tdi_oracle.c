@@ -1127,7 +1127,7 @@ int o_evaluate_f(const o_model *m, const o_frame *f, const o_config *cfg, const 
     if (owner) memcpy(owner, c.fr.owner, N);
     if (image) for (int p = 0; p < NPIX; ++p) image[p] = (float)c.imb[p];
     if (sh) for (int q = 0; q < SH_N; ++q) for (int n = 0; n < N; ++n) sh[(size_t)q * N + n] = (float)c.sh[(size_t)q * N + n];
-    if (grads) for (int q = 0; q < G_N - 1; ++q) for (int n = 0; n < N; ++n) grads[(size_t)q * N + n] = (float)c.g[(size_t)q * N + n];
+    if (grads) for (int q = 0; q < G_N; ++q) for (int n = 0; n < N; ++n) grads[(size_t)q * N + n] = (float)c.g[(size_t)q * N + n];
     if (nb) memcpy(nb, c.nb, sizeof(int32_t) * 4 * N);
     if (J) for (size_t i = 0; i < (size_t)N * KT; ++i) J[i] = (float)c.J[i];
     if (H) for (int i = 0; i < KT * KT; ++i) H[i] = (float)Hr[i];
