@@ -237,7 +237,7 @@ tdi_status geometry(const Launch &L, const Cfg &c, int stage)
     dim3 vg((L.m.V + VT_V - 1) / VT_V, (L.F + VT_F - 1) / VT_F);
     TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, 0, k_precheck, L.fblocks(), dim3(128), 0, L.s, L.m, L.b, c, stage));
-    TDI_TRY(launch(L.bt, KID_RASTER, k_raster, dim3(L.F), dim3(1024), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_RASTER, k_raster, dim3(RC * L.F), dim3(1024), 0, L.s, L.m, L.b));
     return TDI_OK;
 }
 
@@ -251,7 +251,8 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
 {
     TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.F), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
     TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.F), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(L.F), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_SPLIT, L.F), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.F), dim3(NE_THREADS), 0, L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.F), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
     TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.F), dim3(128), L.smem_solve(), L.s, L.m, L.b, c, stage));
@@ -396,9 +397,9 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
-    A(d.ctl, F); A(d.geo, F * 6 * md.V); A(d.zbuf, F * NPIX); A(d.frag, F * NMAX);
+    A(d.ctl, F); A(d.geo, F * 6 * md.V); A(d.zbuf, F * NPIX); A(d.tri_cnt, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
-    A(d.J, F * NMAX * KTP); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
+    A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_SPLIT * (size_t)ne_part_stride((int)KTP)); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
     A(d.prof_frames, 1);
 #undef A
     if (st != TDI_OK) return cleanup(st);
@@ -641,7 +642,7 @@ tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const 
     uint32_t zero = 0;
     TDI_CUDA(cudaMemcpy(&d.ctl[frame].flags, &zero, sizeof(zero), cudaMemcpyHostToDevice));
     TDI_TRY(launch(b, 0, k_set_render, dim3(1), dim3(256), 0, (cudaStream_t)0, d, (int)frame));
-    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(d.F), dim3(1024), 0, (cudaStream_t)0, m, d));
+    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC * d.F), dim3(1024), 0, (cudaStream_t)0, m, d));
     TDI_CUDA(cudaDeviceSynchronize());
     FrameCtl ctl;
     TDI_CUDA(cudaMemcpy(&ctl, d.ctl + frame, sizeof(FrameCtl), cudaMemcpyDeviceToHost));
@@ -665,7 +666,7 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     TDI_TRY(launch(b, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
     dim3 vg((m.V + VT_V - 1) / VT_V, (d.F + VT_F - 1) / VT_F);
     TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
-    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(d.F), dim3(1024), 0, s, m, d));
+    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC * d.F), dim3(1024), 0, s, m, d));
     float *img = d.img;                                   // [F][NPIX] image, then [F][NPIX] map
     int32_t *map = reinterpret_cast<int32_t *>(d.img + (size_t)d.F * NPIX);
     TDI_TRY(launch(b, 0, k_paint, dim3(1, d.F), dim3(1024), 0, s, m, (const DBatch)d, img, map));

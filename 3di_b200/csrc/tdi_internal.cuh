@@ -106,11 +106,13 @@ struct DBatch {
     // per-render working set
     float *geo;              // [F][6][V]: X0, Y0, Z0, xp, yp, Zc
     unsigned long long *zbuf;// [F][NPIX]
+    uint8_t *tri_cnt;        // [F][T] fragments of each triangle in the last raster
     Fragment *frag;          // [F][NMAX]
     float *fgrad;            // [F][5][NMAX]: gx, gy, h, gxs_n, gys_n
     int32_t *nb;             // [F][4][NMAX]: kl, kr, ka, kb
     int32_t *perm;           // [F][NMAX]: sorted position -> fragment
     float *J;                // [F][NMAX][KTP]
+    double *ne_part;         // [F][NE_SPLIT][part stride] partial normal equations
     float *img;              // [F][2][NPIX] blur scratch for frames too large for shared memory
     // live profiling: frames processed by the kernel being timed (kernel ids as in tdi.h)
     unsigned long long *prof_frames;

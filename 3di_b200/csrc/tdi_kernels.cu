@@ -3,6 +3,7 @@
 // contraction, so each per-fragment quantity is bit-identical to the CPU oracle's.
 #include "tdi_internal.cuh"
 
+#include <cooperative_groups.h>
 #include <cfloat>
 #include <cmath>
 
@@ -383,52 +384,65 @@ __device__ __forceinline__ unsigned long long zkey(uint32_t tag, float Z, int tr
            (unsigned long long)(uint32_t)tri;
 }
 
-__global__ void __launch_bounds__(1024) k_raster(DModel m, DBatch b)
+// One thread-block cluster of RC blocks per frame. Warps own consecutive ranges of
+// triangles (lanes take consecutive triangles), so slot order is warp order within a block,
+// block rank order within the cluster, and row r order across the frame.
+constexpr int RC = 8;                       // blocks per frame (cluster size)
+constexpr int RWARPS = 32;                  // warps per block
+
+__device__ __forceinline__ bool survives(unsigned long long k, uint32_t tag, uint32_t zbits)
 {
-    const int f = blockIdx.x;
+    return (uint32_t)(k >> (31 + TRI_BITS)) == tag && (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zbits;
+}
+
+__global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DModel m, DBatch b)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int f = blockIdx.x / RC;
+    const int rank = (int)cluster.block_rank();
     FrameCtl &ctl = b.ctl[f];
-    if (!ctl.render) return;
-    if (threadIdx.x == 0) prof_count(b, KID_RASTER);
-    __shared__ uint32_t s_cnt[32][NTMP];
-    __shared__ uint32_t s_off[32][NTMP];
+    if (!ctl.render) return;                 // the whole cluster belongs to this frame
+    if (threadIdx.x == 0 && rank == 0) prof_count(b, KID_RASTER);
+    __shared__ uint32_t s_cnt[RWARPS][NTMP];   // survivors per warp and row
+    __shared__ uint32_t s_off[RWARPS][NTMP];   // exclusive offsets within the block
+    __shared__ uint32_t s_blk[NTMP];           // this block's totals per row (read by the cluster)
     __shared__ int s_bbox[4];
     __shared__ uint32_t s_flags;
-    __shared__ uint32_t s_tag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long *zb = b.zbuf + (size_t)f * NPIX;
+    uint8_t *cnt8 = b.tri_cnt + (size_t)f * m.T;
+    uint32_t epoch = ctl.epoch + 1;
+    const bool wrap = epoch > TAG_MAX;
+    if (wrap) epoch = 1;
     if (tid == 0) {
-        uint32_t e = ctl.epoch + 1;
-        if (e > TAG_MAX) e = 0;           // wrap: clear below, restart the epochs
-        s_tag = e;
         s_flags = 0;
         s_bbox[0] = s_bbox[2] = 1 << 30;
         s_bbox[1] = s_bbox[3] = -1;
     }
-    __syncthreads();
-    if (s_tag == 0) {
-        for (int p = tid; p < NPIX; p += 1024) zb[p] = ~0ull;
-        __syncthreads();
-        if (tid == 0) s_tag = 1;
-        __syncthreads();
-    }
-    const uint32_t epoch = s_tag;
+    if (wrap)
+        for (int p = rank * 1024 + tid; p < NPIX; p += RC * 1024) zb[p] = ~0ull;
+    __threadfence();
+    cluster.sync();
     const uint32_t tag = TAG_MAX - epoch;
     const float *geo = b.geo + (size_t)f * 6 * m.V;
     const float *xp = geo + 3 * m.V, *yp = geo + 4 * m.V, *Zc = geo + 5 * m.V;
     const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
     const int T = m.T;
-    const int per_warp = ((T + 32 * 32 - 1) / (32 * 32)) * 32;
-    const int t_begin = warp * per_warp;
+    const int gwarps = RC * RWARPS;
+    const int per_warp = ((T + gwarps * 32 - 1) / (gwarps * 32)) * 32;
+    const int t_begin = (rank * RWARPS + warp) * per_warp;
     const int t_end = min(T, t_begin + per_warp);
     uint32_t flags = 0;
     int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
 
-    // pass A: depth keys
+    // pass A: depth keys, fragment count per triangle
     for (int base = t_begin; base < t_end; base += 32) {
         const int idx = base + lane;
         if (idx < t_end) {
             uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
             const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, flags);
+            cnt8[idx] = (uint8_t)nf;
             if (nf) {
                 const float Z = Zc[m.tl[idx]];
                 if (!(Z > 0.0f)) flags |= FLAG_OUT_OF_DOMAIN;
@@ -437,50 +451,55 @@ __global__ void __launch_bounds__(1024) k_raster(DModel m, DBatch b)
             }
         }
     }
-    __syncthreads();
+    __threadfence();
+    cluster.sync();
 
-    // pass B: survivors per slot row
+    // pass B: survivors per row, warp and block
     uint32_t cnt[NTMP] = {0, 0, 0, 0};
     for (int base = t_begin; base < t_end; base += 32) {
         const int idx = base + lane;
-        bool s[NTMP] = {false, false, false, false};
-        if (idx < t_end) {
+        bool sv[NTMP] = {false, false, false, false};
+        if (idx < t_end && cnt8[idx]) {
             uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
             uint32_t fl2 = 0;
             const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
-            if (nf) {
-                const float Z = Zc[m.tl[idx]];
-                const uint32_t zb_bits = __float_as_uint(Z) & 0x7FFFFFFFu;
-                for (int r = 0; r < nf; ++r) {
-                    const unsigned long long k = __ldcg(zb + pix[r]);
-                    const bool live = (uint32_t)(k >> (31 + TRI_BITS)) == tag &&
-                                      (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zb_bits;
-                    s[r] = live && !(r == 0 && idx == 0);
-                }
-            }
+            const uint32_t zbits = __float_as_uint(Zc[m.tl[idx]]) & 0x7FFFFFFFu;
+            for (int r = 0; r < nf; ++r)
+                sv[r] = survives(__ldcg(zb + pix[r]), tag, zbits) && !(r == 0 && idx == 0);
         }
 #pragma unroll
-        for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, s[r]));
+        for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
     }
     if (lane == 0)
         for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
     __syncthreads();
     if (tid < NTMP) {
-        // exclusive scan over warps for row r; rows follow each other
         uint32_t tot = 0;
-        for (int w = 0; w < 32; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
-        s_cnt[0][tid] = tot;     // reuse: row totals (read after the barrier below)
+        for (int w = 0; w < RWARPS; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
+        s_blk[tid] = tot;
     }
-    __syncthreads();
-    uint32_t rowbase[NTMP];
+    cluster.sync();
+    // frame totals per row and the offset of this block within each row
+    uint32_t rowbase[NTMP], blkoff[NTMP];
     {
+        uint32_t tot[NTMP] = {0, 0, 0, 0};
+        for (int q = 0; q < RC; ++q) {
+            const uint32_t *rb = cluster.map_shared_rank(s_blk, q);
+            for (int r = 0; r < NTMP; ++r) {
+                const uint32_t v = rb[r];
+                if (q == rank) blkoff[r] = tot[r];
+                tot[r] += v;
+            }
+        }
         uint32_t acc = 0;
-        for (int r = 0; r < NTMP; ++r) { rowbase[r] = acc; acc += s_cnt[0][r]; }
-        if (tid == 0) {
+        for (int r = 0; r < NTMP; ++r) { rowbase[r] = acc; acc += tot[r]; }
+        if (tid == 0 && rank == 0) {
             ctl.N = (int)min(acc, (uint32_t)NMAX);
-            if (acc > (uint32_t)NMAX) atomicOr(&s_flags, FLAG_OVERFLOW);
-            if (acc < 1000u || acc > 52000u) atomicOr(&s_flags, FLAG_RENDER_SKIPPED);
-            if (acc > 25600u) atomicOr(&s_flags, FLAG_OUT_OF_DOMAIN);
+            uint32_t fl = 0;
+            if (acc > (uint32_t)NMAX) fl |= FLAG_OVERFLOW;
+            if (acc < 1000u || acc > 52000u) fl |= FLAG_RENDER_SKIPPED;
+            if (acc > 25600u) fl |= FLAG_OUT_OF_DOMAIN;
+            atomicOr(&s_flags, fl);
         }
     }
 
@@ -490,31 +509,26 @@ __global__ void __launch_bounds__(1024) k_raster(DModel m, DBatch b)
     Fragment *out = b.frag + (size_t)f * NMAX;
     for (int base = t_begin; base < t_end; base += 32) {
         const int idx = base + lane;
-        bool s[NTMP] = {false, false, false, false};
+        bool sv[NTMP] = {false, false, false, false};
         bool own[NTMP] = {false, false, false, false};
         uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-        int nf = 0;
-        if (idx < t_end) {
+        if (idx < t_end && cnt8[idx]) {
             uint32_t fl2 = 0;
-            nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
-            if (nf) {
-                const float Z = Zc[m.tl[idx]];
-                const uint32_t zb_bits = __float_as_uint(Z) & 0x7FFFFFFFu;
-                const unsigned long long mykey = zkey(tag, Z, idx);
-                for (int r = 0; r < nf; ++r) {
-                    const unsigned long long k = __ldcg(zb + pix[r]);
-                    const bool live = (uint32_t)(k >> (31 + TRI_BITS)) == tag &&
-                                      (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zb_bits;
-                    s[r] = live && !(r == 0 && idx == 0);
-                    own[r] = (k == mykey);
-                }
+            const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
+            const float Z = Zc[m.tl[idx]];
+            const uint32_t zbits = __float_as_uint(Z) & 0x7FFFFFFFu;
+            const unsigned long long mykey = zkey(tag, Z, idx);
+            for (int r = 0; r < nf; ++r) {
+                const unsigned long long k = __ldcg(zb + pix[r]);
+                sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
+                own[r] = (k == mykey);
             }
         }
 #pragma unroll
         for (int r = 0; r < NTMP; ++r) {
-            const unsigned mask = __ballot_sync(0xffffffffu, s[r]);
-            if (s[r]) {
-                const uint32_t pos = rowbase[r] + s_off[warp][r] + run[r] + __popc(mask & lt_mask);
+            const unsigned mask = __ballot_sync(0xffffffffu, sv[r]);
+            if (sv[r]) {
+                const uint32_t pos = rowbase[r] + blkoff[r] + s_off[warp][r] + run[r] + __popc(mask & lt_mask);
                 if (pos < (uint32_t)NMAX) {
                     Fragment fr;
                     fr.pix_owner = (uint32_t)pix[r] | (own[r] ? 0x80000000u : 0u);
@@ -535,16 +549,25 @@ __global__ void __launch_bounds__(1024) k_raster(DModel m, DBatch b)
         atomicMin(&s_bbox[0], bx0); atomicMax(&s_bbox[1], bx1);
         atomicMin(&s_bbox[2], by0); atomicMax(&s_bbox[3], by1);
     }
-    __syncthreads();
-    if (tid == 0) {
+    cluster.sync();
+    if (tid == 0 && rank == 0) {
+        int bb[4] = {1 << 30, -1, 1 << 30, -1};
+        uint32_t fl = 0;
+        for (int q = 0; q < RC; ++q) {
+            const int *rb = cluster.map_shared_rank(s_bbox, q);
+            bb[0] = min(bb[0], rb[0]); bb[1] = max(bb[1], rb[1]);
+            bb[2] = min(bb[2], rb[2]); bb[3] = max(bb[3], rb[3]);
+            fl |= *cluster.map_shared_rank(&s_flags, q);
+        }
         ctl.epoch = epoch;
-        ctl.flags |= s_flags;
+        ctl.flags |= fl;
         ctl.renders += 1;
-        for (int q = 0; q < 4; ++q) ctl.bbox[q] = s_bbox[q];
-        if (s_bbox[1] >= 0 && (s_bbox[0] < 1 || s_bbox[1] > DIM - 2 || s_bbox[2] < 1 || s_bbox[3] > DIM - 2))
+        for (int q = 0; q < 4; ++q) ctl.bbox[q] = bb[q];
+        if (bb[1] >= 0 && (bb[0] < 1 || bb[1] > DIM - 2 || bb[2] < 1 || bb[3] > DIM - 2))
             ctl.flags |= FLAG_OUT_OF_DOMAIN;
-        if (s_flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) ctl.render = 0;
+        if (fl & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) ctl.render = 0;
     }
+    cluster.sync();   // keep shared memory alive until rank 0 has read it
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1025,28 +1048,40 @@ __device__ __forceinline__ void chain(const float *Jf, int ld, const int32_t *nb
 // accumulation (4x4 register blocks of the upper triangle per thread).
 
 constexpr int NE_THREADS = 256, NE_CHUNK = 32;
+constexpr int NE_SPLIT = 16;                 // blocks per frame, each over a range of fragments
 
+// Upper-triangle 4x4 block (bi <= bj) owned by thread t, or -1.
+__device__ __forceinline__ void ne_block(int t, int nb4, int &bi, int &bj)
+{
+    bi = bj = -1;
+    for (int i = 0; i < nb4 && bi < 0; ++i) {
+        const int len = nb4 - i;
+        if (t < len) { bi = i; bj = i + t; } else t -= len;
+    }
+}
+
+__host__ __device__ __forceinline__ int ne_part_stride(int KTP)
+{
+    const int nb4 = KTP / 4;
+    return nb4 * (nb4 + 1) / 2 * 16 + KTP;
+}
+
+// Partial sums of one fragment range: sum(row row^T) for the upper 4x4 blocks and
+// sum(w row), FP64, written to b.ne_part[f][split].
 __global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
 {
-    const int f = blockIdx.x;
+    const int f = blockIdx.y, split = blockIdx.x;
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
-    if (threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
+    if (split == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
     extern __shared__ float nesm[];
     const int KTP = m.KTP, KT = m.KT;
     float *rows = nesm;                          // [2*NE_CHUNK][KTP]
     float *wts = rows + 2 * NE_CHUNK * KTP;      // [2*NE_CHUNK]
     const int tid = threadIdx.x;
     const int nb4 = KTP / 4;
-    // upper-triangle 4x4 block owned by this thread
-    int bi = -1, bj = -1;
-    {
-        int t = tid;
-        for (int i = 0; i < nb4 && bi < 0; ++i) {
-            const int len = nb4 - i;
-            if (t < len) { bi = i; bj = i + t; } else t -= len;
-        }
-    }
+    int bi, bj;
+    ne_block(tid, nb4, bi, bj);
     double acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -1054,11 +1089,13 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
     double gacc = 0.0;
     const int N = ctl.N;
+    const int per = ((N + NE_SPLIT * NE_CHUNK - 1) / (NE_SPLIT * NE_CHUNK)) * NE_CHUNK;
+    const int nbeg = split * per, nend = min(N, nbeg + per);
     const float *Jf = b.J + (size_t)f * NMAX * KTP;
     const int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
     const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
-    for (int n0 = 0; n0 < N; n0 += NE_CHUNK) {
-        const int cn = min(NE_CHUNK, N - n0);
+    for (int n0 = nbeg; n0 < nend; n0 += NE_CHUNK) {
+        const int cn = min(NE_CHUNK, nend - n0);
         for (int i = tid; i < NE_CHUNK * KTP; i += NE_THREADS) {
             const int q = i / KTP, j = i - q * KTP;
             float ox = 0.0f, oy = 0.0f;
@@ -1097,19 +1134,45 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
         }
         __syncthreads();
     }
+    const int stride = ne_part_stride(KTP);
+    double *part = b.ne_part + ((size_t)f * NE_SPLIT + split) * stride;
+    if (bi >= 0)
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) part[tid * 16 + i * 4 + j] = acc[i][j];
+    if (tid < KTP) part[nb4 * (nb4 + 1) / 2 * 16 + tid] = gacc;
+}
+
+// Sum of the partial normal equations in split order: H = tau*S, g = -tau*w.
+__global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatch b)
+{
+    const int f = blockIdx.x;
+    const FrameCtl &ctl = b.ctl[f];
+    if (!ctl.need_jac) return;
+    const int KTP = m.KTP, KT = m.KT, tid = threadIdx.x;
+    const int nb4 = KTP / 4;
+    const int stride = ne_part_stride(KTP);
+    const double *part = b.ne_part + (size_t)f * NE_SPLIT * stride;
     const double tau = 25.0;
     float *H = b.H + (size_t)f * KTP * KTP;
+    int bi, bj;
+    ne_block(tid, nb4, bi, bj);
     if (bi >= 0) {
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 4; ++j) {
+                double s = 0.0;
+                for (int q = 0; q < NE_SPLIT; ++q) s += part[(size_t)q * stride + tid * 16 + i * 4 + j];
                 const int a = 4 * bi + i, c = 4 * bj + j;
                 if (a >= KT || c >= KT) continue;
-                const float v = (float)(tau * acc[i][j]);
+                const float v = (float)(tau * s);
                 H[(size_t)a * KTP + c] = v;
                 H[(size_t)c * KTP + a] = v;
             }
     }
-    if (tid < KT) b.g[(size_t)f * KTP + tid] = (float)(-tau * gacc);
+    if (tid < KT) {
+        double s = 0.0;
+        for (int q = 0; q < NE_SPLIT; ++q) s += part[(size_t)q * stride + nb4 * (nb4 + 1) / 2 * 16 + tid];
+        b.g[(size_t)f * KTP + tid] = (float)(-tau * s);
+    }
 }
 
 // ------------------------------------------------------------------------------------------
