@@ -90,6 +90,9 @@ SIGNATURES = {
     "tdi_batch_profile": (C.c_int32, [C.c_void_p, C.c_int32]),
     "tdi_batch_profile_read": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                            C.POINTER(C.c_int64)]),
+    "tdi_raster_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 KERNEL_IDS = dict(vertex=1, raster=2, render=3, neighbours=4, jacobian=5, normal_eq=6, barrier=7,

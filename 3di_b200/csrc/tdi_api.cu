@@ -713,3 +713,5 @@ tdi_status tdi_batch_profile_read(tdi_batch *b, int64_t *launches, double *total
 }
 
 }  // extern "C"
+
+#include "tdi_noalloc.cu"

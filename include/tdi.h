@@ -170,6 +170,22 @@ tdi_status tdi_batch_profile(tdi_batch *b, int32_t kernel_id);
 tdi_status tdi_batch_profile_read(tdi_batch *b, int64_t *launches, double *total_ms,
                                   int64_t *frames);
 
+/* Visibility of one frame for callers that cannot allocate device memory (no counterpart in
+ * 3DI, which allocates all of its working memory up front). Same result as tdi_batch_raster
+ * for the same projections: device arrays xp, yp, camera Z [n_vertices], triangles
+ * [3][n_triangles] (0-based), crop origin; output: fragments int32 [capacity][4] (pixel |
+ * owner<<31, triangle, float bits of alpha, beta) in slot order, *count (device int32, the
+ * number written) and *flags (device uint32, TDI_FLAG_*). Calls no allocator: its working
+ * memory is a fixed 640 KiB array in the library's device image, held on every device that
+ * loads the library until the process exits. At most 131,072 triangles (TDI_ERR_CAPACITY
+ * otherwise). Calls share that array: calls that overlap on the GPU race; serialise them on
+ * one stream. The first call on a device looks the array up (cudaGetSymbolAddress) with that
+ * device current, so make it before any stream capture. Asynchronous on the stream. */
+tdi_status tdi_raster_noalloc(const float *xp, const float *yp, const float *zc,
+                              const int32_t *triangles, int32_t n_vertices, int32_t n_triangles,
+                              int32_t x0, int32_t y0, int32_t *fragments, int32_t capacity,
+                              int32_t *count, uint32_t *flags, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
