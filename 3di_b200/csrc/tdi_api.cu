@@ -10,6 +10,7 @@
 
 #include "../../include/tdi.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -214,6 +215,7 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_barrier_full, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_precheck, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     done = true;
     return TDI_OK;
 }
@@ -230,32 +232,47 @@ struct Launch {
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
     size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
     dim3 fblocks() const { return dim3((F + 127) / 128); }
+    int A() const { return b.nact; }                      // frames active this round
+    dim3 ablocks() const { return dim3((A() + 127) / 128); }
 };
+
+// Compacts the list of frames running the stage and returns how many there are (one 4-byte
+// read-back per call).
+tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
+{
+    TDI_TRY(launch(bt, 0, k_compact_active, dim3(1), dim3(1024), 0, s, (const DBatch)bt->d, bt->d_count));
+    TDI_CUDA(cudaMemcpyAsync(bt->h_count, bt->d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    *n = *bt->h_count;
+    bt->d.nact = *n;
+    return TDI_OK;
+}
 
 tdi_status geometry(const Launch &L, const Cfg &c, int stage)
 {
-    dim3 vg((L.m.V + VT_V - 1) / VT_V, (L.F + VT_F - 1) / VT_F);
+    dim3 vg((L.m.V + VT_V - 1) / VT_V, (L.A() + VT_F - 1) / VT_F);
     TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, 0, k_precheck, L.fblocks(), dim3(128), 0, L.s, L.m, L.b, c, stage));
-    TDI_TRY(launch(L.bt, KID_RASTER, k_raster, dim3(RC * L.F), dim3(1024), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
+                   (size_t)PC_WARPS * (2 * L.m.K + 4 * NL) * sizeof(float), L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, KID_RASTER, k_raster, dim3(RC * L.A()), dim3(1024), 0, L.s, L.m, L.b));
     return TDI_OK;
 }
 
 tdi_status render(const Launch &L, const Cfg &c, int stage)
 {
-    return launch(L.bt, KID_RENDER, k_render, dim3(L.F), dim3(RENDER_THREADS),
+    return launch(L.bt, KID_RENDER, k_render, dim3(L.A()), dim3(RENDER_THREADS),
                   RENDER_SMEM_FLOATS * sizeof(float), L.s, L.m, L.b, c, stage);
 }
 
 tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
 {
-    TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.F), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
-    TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.F), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_SPLIT, L.F), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.F), dim3(NE_THREADS), 0, L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.F), dim3(256), L.smem_bar(), L.s, L.m, L.b,
+    TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
+    TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.A()), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_SPLIT, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
-    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.F), dim3(128), L.smem_solve(), L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(128), L.smem_solve(), L.s, L.m, L.b, c, stage));
     return TDI_OK;
 }
 
@@ -265,28 +282,27 @@ tdi_status run_stage(tdi_batch *bt, const Cfg &c, int stage, cudaStream_t s)
     const DBatch &b = bt->d;
     Launch L{bt, m, b, s, b.F};
     TDI_TRY(launch(bt, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, b, c, stage));
+    int n = 0;
+    TDI_TRY(compact_active(bt, s, &n));
     const long max_rounds = stage == ST_LAMBDA ? 8L * c.max_iters_lambda + 16
                                                : 16L * (stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune) + 16;
-    for (long round = 0; round < max_rounds; ++round) {
-        TDI_TRY(launch(bt, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, b, stage));
+    for (long round = 0; round < max_rounds && n > 0; ++round) {
+        TDI_TRY(launch(bt, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, b, stage));
         if (stage == ST_LAMBDA) {
             if (round == 0) {
                 TDI_TRY(geometry(L, c, stage));
-                TDI_TRY(launch(bt, KID_NEIGHBOURS, k_neighbours, dim3(L.F), dim3(1024), L.smem_neigh(), s, b, 1));
+                TDI_TRY(launch(bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), s, b, 1));
             }
             TDI_TRY(render(L, c, stage));
-            TDI_TRY(launch(bt, 0, k_decide_lambda, L.fblocks(), dim3(128), 0, s, m, b, c));
-            TDI_TRY(launch(bt, 0, k_lambda_jac, dim3(L.F), dim3(256), 0, s, m, b, c));
+            TDI_TRY(launch(bt, 0, k_decide_lambda, L.ablocks(), dim3(128), 0, s, m, b, c));
+            TDI_TRY(launch(bt, 0, k_lambda_jac, dim3(L.A()), dim3(256), 0, s, m, b, c));
         } else {
             TDI_TRY(geometry(L, c, stage));
             TDI_TRY(render(L, c, stage));
-            TDI_TRY(launch(bt, 0, k_decide_shape, L.fblocks(), dim3(128), 0, s, m, b, c, stage));
+            TDI_TRY(launch(bt, 0, k_decide_shape, L.ablocks(), dim3(128), 0, s, m, b, c, stage));
             TDI_TRY(normal_equations(L, c, stage));
         }
-        TDI_TRY(launch(bt, 0, k_count_active, dim3(1), dim3(256), 0, s, b, bt->d_count));
-        TDI_CUDA(cudaMemcpyAsync(bt->h_count, bt->d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
-        TDI_CUDA(cudaStreamSynchronize(s));
-        if (*bt->h_count == 0) break;
+        TDI_TRY(compact_active(bt, s, &n));
     }
     return TDI_OK;
 }
@@ -337,13 +353,44 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
     DModel &d = m->d;
     d.V = V; d.T = T; d.K = K; d.KP = round4(K); d.KT = K + 6; d.KTP = round4(K + 6);
     float *mean, *E, *tex, *epsb;
-    int32_t *tl, *lis;
+    int32_t *tl, *lis, *order;
     auto cleanup = [&](tdi_status st) { for (void *p : m->allocs) cudaFree(p); delete m; return st; };
     tdi_status st;
     if ((st = dalloc(m->allocs, &mean, 3 * (size_t)V)) || (st = dalloc(m->allocs, &E, (size_t)V * 3 * d.KP)) ||
         (st = dalloc(m->allocs, &tex, (size_t)V)) || (st = dalloc(m->allocs, &tl, 3 * (size_t)T)) ||
-        (st = dalloc(m->allocs, &lis, (size_t)NL)) || (st = dalloc(m->allocs, &epsb, 4 * (size_t)K)))
+        (st = dalloc(m->allocs, &lis, (size_t)NL)) || (st = dalloc(m->allocs, &epsb, 4 * (size_t)K)) ||
+        (st = dalloc(m->allocs, &order, (size_t)T)))
         return cleanup(st);
+    // Visiting order of the raster's depth pass: Morton order of the triangle centroids in
+    // the mean shape's x-y plane (the z-buffer result does not depend on the order).
+    std::vector<int32_t> tord(T);
+    {
+        float xmin = desc->mean[0], xmax = xmin, ymin = desc->mean[V], ymax = ymin;
+        for (int v = 0; v < V; ++v) {
+            xmin = std::min(xmin, desc->mean[v]); xmax = std::max(xmax, desc->mean[v]);
+            ymin = std::min(ymin, desc->mean[V + v]); ymax = std::max(ymax, desc->mean[V + v]);
+        }
+        std::vector<std::pair<uint32_t, int32_t>> keys(T);
+        auto spread = [](uint32_t x) {
+            x &= 0xFFFF;
+            x = (x | (x << 8)) & 0x00FF00FFu; x = (x | (x << 4)) & 0x0F0F0F0Fu;
+            x = (x | (x << 2)) & 0x33333333u; x = (x | (x << 1)) & 0x55555555u;
+            return x;
+        };
+        const float sx = 65535.0f / std::max(xmax - xmin, 1e-20f), sy = 65535.0f / std::max(ymax - ymin, 1e-20f);
+        for (int t = 0; t < T; ++t) {
+            float cx = 0.0f, cy = 0.0f;
+            for (int r = 0; r < 3; ++r) {
+                const int v = desc->triangles[r * T + t];
+                cx += desc->mean[v]; cy += desc->mean[V + v];
+            }
+            const uint32_t qx = (uint32_t)std::min(65535.0f, std::max(0.0f, (cx / 3.0f - xmin) * sx));
+            const uint32_t qy = (uint32_t)std::min(65535.0f, std::max(0.0f, (cy / 3.0f - ymin) * sy));
+            keys[t] = {spread(qx) | (spread(qy) << 1), t};
+        }
+        std::sort(keys.begin(), keys.end());
+        for (int t = 0; t < T; ++t) tord[t] = keys[t].second;
+    }
     std::vector<float> Ep((size_t)V * 3 * d.KP, 0.0f);
     for (size_t r = 0; r < (size_t)V * 3; ++r)
         std::memcpy(&Ep[r * d.KP], desc->expr_basis + r * K, sizeof(float) * K);
@@ -357,9 +404,10 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
         cudaMemcpy(tex, desc->tex, sizeof(float) * V, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(tl, desc->triangles, sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(lis, desc->landmarks, sizeof(int32_t) * NL, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(epsb, eb.data(), sizeof(float) * eb.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(epsb, eb.data(), sizeof(float) * eb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(order, tord.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice) != cudaSuccess)
         return cleanup(fail(TDI_ERR_CUDA, "model upload failed"));
-    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb;
+    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb; d.tri_order = order;
     *out = m;
     return TDI_OK;
 }
@@ -397,7 +445,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
-    A(d.ctl, F); A(d.geo, F * 6 * md.V); A(d.zbuf, F * NPIX); A(d.tri_cnt, F * (size_t)md.T); A(d.frag, F * NMAX);
+    A(d.ctl, F); A(d.act, F); A(d.geo, F * 6 * md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_cnt, F * (size_t)md.T); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
     A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_SPLIT * (size_t)ne_part_stride((int)KTP)); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
     A(d.prof_frames, 1);
@@ -557,10 +605,13 @@ tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t f
     TDI_TRY(blur_targets(b, c, s));
     TDI_TRY(launch(b, 0, k_fit_begin, L.fblocks(), dim3(128), 0, s, d));
     TDI_TRY(launch(b, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, d, c, stage));
-    TDI_TRY(launch(b, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, d, stage));
+    int n = 0;
+    TDI_TRY(compact_active(b, s, &n));
+    if (n == 0) return TDI_OK;
+    TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, stage));
     TDI_TRY(geometry(L, c, stage));
     TDI_TRY(render(L, c, stage));
-    TDI_TRY(launch(b, 0, k_decide_shape, L.fblocks(), dim3(128), 0, s, m, d, c, stage));
+    TDI_TRY(launch(b, 0, k_decide_shape, L.ablocks(), dim3(128), 0, s, m, d, c, stage));
     TDI_TRY(normal_equations(L, c, stage));
     TDI_TRY(launch(b, 0, k_scalars, L.fblocks(), dim3(128), 0, s, d, b->scalars));
     TDI_CUDA(cudaStreamSynchronize(s));
@@ -617,7 +668,11 @@ tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, 
         break;
     case 6:
         if (capacity < (int64_t)(6 * (size_t)m.V * sizeof(float))) return fail(TDI_ERR_INVALID, "destination too small");
-        TDI_CUDA(cudaMemcpy(dst, d.geo + (size_t)frame * 6 * m.V, 6 * (size_t)m.V * sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(dst, d.geo + (size_t)frame * 6 * m.V, 3 * (size_t)m.V * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 3; ++c)
+            TDI_CUDA(cudaMemcpy2D(static_cast<float *>(dst) + (3 + c) * (size_t)m.V, sizeof(float),
+                                  reinterpret_cast<const float *>(d.proj + (size_t)frame * m.V) + c, sizeof(float4),
+                                  sizeof(float), m.V, cudaMemcpyDeviceToHost));
         n = 6 * (int64_t)m.V;
         break;
     default:
@@ -633,16 +688,17 @@ tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const 
     if (!b || !xp || !yp || !zc || frame < 0 || frame >= b->d.F) return fail(TDI_ERR_INVALID, "bad raster arguments");
     const DModel &m = b->m->d;
     DBatch &d = b->d;
-    float *g = d.geo + (size_t)frame * 6 * m.V;
-    TDI_CUDA(cudaMemcpy(g + 3 * (size_t)m.V, xp, sizeof(float) * m.V, cudaMemcpyHostToDevice));
-    TDI_CUDA(cudaMemcpy(g + 4 * (size_t)m.V, yp, sizeof(float) * m.V, cudaMemcpyHostToDevice));
-    TDI_CUDA(cudaMemcpy(g + 5 * (size_t)m.V, zc, sizeof(float) * m.V, cudaMemcpyHostToDevice));
+    std::vector<float4> pj(m.V);
+    for (int v = 0; v < m.V; ++v) pj[v] = make_float4(xp[v], yp[v], zc[v], 0.0f);
+    TDI_CUDA(cudaMemcpy(d.proj + (size_t)frame * m.V, pj.data(), sizeof(float4) * m.V, cudaMemcpyHostToDevice));
     int32_t o[2] = {x0, y0};
     TDI_CUDA(cudaMemcpy((void *)(d.x0y0 + 2 * frame), o, sizeof(o), cudaMemcpyHostToDevice));
     uint32_t zero = 0;
     TDI_CUDA(cudaMemcpy(&d.ctl[frame].flags, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    TDI_CUDA(cudaMemcpy(d.act, &frame, sizeof(int32_t), cudaMemcpyHostToDevice));
+    d.nact = 1;
     TDI_TRY(launch(b, 0, k_set_render, dim3(1), dim3(256), 0, (cudaStream_t)0, d, (int)frame));
-    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC * d.F), dim3(1024), 0, (cudaStream_t)0, m, d));
+    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC), dim3(1024), 0, (cudaStream_t)0, m, d));
     TDI_CUDA(cudaDeviceSynchronize());
     FrameCtl ctl;
     TDI_CUDA(cudaMemcpy(&ctl, d.ctl + frame, sizeof(FrameCtl), cudaMemcpyDeviceToHost));
@@ -663,10 +719,14 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     // evaluation point = x (shape-fit full evaluation), no fitting
     TDI_TRY(launch(b, 0, k_fit_begin, L.fblocks(), dim3(128), 0, s, d));
     TDI_TRY(launch(b, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, d, c, (int)ST_RIGID));
-    TDI_TRY(launch(b, 0, k_prepare, L.fblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
-    dim3 vg((m.V + VT_V - 1) / VT_V, (d.F + VT_F - 1) / VT_F);
-    TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
-    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC * d.F), dim3(1024), 0, s, m, d));
+    int n = 0;
+    TDI_TRY(compact_active(b, s, &n));
+    if (n > 0) {
+        TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
+        dim3 vg((m.V + VT_V - 1) / VT_V, (n + VT_F - 1) / VT_F);
+        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
+        TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC * n), dim3(1024), 0, s, m, d));
+    }
     float *img = d.img;                                   // [F][NPIX] image, then [F][NPIX] map
     int32_t *map = reinterpret_cast<int32_t *>(d.img + (size_t)d.F * NPIX);
     TDI_TRY(launch(b, 0, k_paint, dim3(1, d.F), dim3(1024), 0, s, m, (const DBatch)d, img, map));

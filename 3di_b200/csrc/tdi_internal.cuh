@@ -83,6 +83,7 @@ struct DModel {
     const int32_t *tl;       // [3][T]
     const int32_t *lis;      // [NL]
     const float *eps_b;      // [4][K]: lb, ub, lb_ft, ub_ft
+    const int32_t *tri_order;// [T] triangles in Morton order of their mean-shape centroids
 };
 
 // Device view of a batch of frames and its working set.
@@ -103,10 +104,14 @@ struct DBatch {
     float *H;                // [F][KTP][KTP]
     float *R, *dR;           // [F][9], [F][27] of the evaluation point
     FrameCtl *ctl;           // [F]
+    int32_t *act;            // [F] frames running the stage at the start of the round, ascending
+    int32_t nact;            // entries of act
     // per-render working set
-    float *geo;              // [F][6][V]: X0, Y0, Z0, xp, yp, Zc
+    float *geo;              // [F][6][V]: X0, Y0, Z0 planes (planes 3-5 unused)
+    float4 *proj;            // [F][V]: xp, yp, camera Z, 0 -- what the raster gathers
     unsigned long long *zbuf;// [F][NPIX]
     uint8_t *tri_cnt;        // [F][T] fragments of each triangle in the last raster
+    int32_t *tri_list;       // [F][T] triangles with fragments, ascending
     Fragment *frag;          // [F][NMAX]
     float *fgrad;            // [F][5][NMAX]: gx, gy, h, gxs_n, gys_n
     int32_t *nb;             // [F][4][NMAX]: kl, kr, ka, kb

@@ -150,8 +150,9 @@ __global__ void k_stage_start(DModel m, DBatch b, Cfg c, int stage)
 // Evaluation point, rotation and render flag of every active frame.
 __global__ void k_prepare(DModel m, DBatch b, int stage)
 {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.F) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b.nact) return;
+    const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     ctl.need_jac = 0;
     if (!ctl.active) { ctl.render = 0; return; }
@@ -165,22 +166,22 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 // ------------------------------------------------------------------------------------------
 // Vertex stage: X0 = mean + E*eps (sequential fmaf over k), camera transform and
 // projection (renderer.cu:806-861, funcs.cu:395-453) for a tile of 32 vertices x 32 frames.
-// geo[f] = [X0 | Y0 | Z0 | xp | yp | Zc] planes of V floats.
+// geo[f] = [X0 | Y0 | Z0] planes of V floats; proj[f][v] = (xp, yp, camera Z, 0).
 
-constexpr int VT_V = 32, VT_F = 32, VT_FPT = 4;   // vertices, frames per block; frames per thread
+constexpr int VT_V = 32, VT_FPT = 8, VT_F = 8 * VT_FPT;   // vertices, frames per block; frames per thread
 
 __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
 {
     extern __shared__ float vsm[];
     const int KP = m.KP, K = m.K;
-    float *Es = vsm;                           // [3*KP][33]
-    float *Xs = vsm + 3 * KP * 33;             // [VT_F][KP]
+    float *Es = vsm;                           // [3*KP][33]: basis rows, vertex-minor
+    float *Xs = vsm + 3 * KP * 33;             // [VT_F][KP]: coefficients per frame
     __shared__ int s_any;
     const int v0 = blockIdx.x * VT_V, f0 = blockIdx.y * VT_F;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     if (tid == 0) s_any = 0;
     __syncthreads();
-    if (tid < VT_F && f0 + tid < b.F && b.ctl[f0 + tid].render) {
+    if (tid < VT_F && f0 + tid < b.nact && b.ctl[b.act[f0 + tid]].render) {
         s_any = 1;
         if (blockIdx.x == 0) prof_count(b, KID_VERTEX);
     }
@@ -193,8 +194,8 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
     }
     for (int i = tid; i < VT_F * KP; i += 256) {
         int fl = i / KP, k = i - fl * KP;
-        int f = f0 + fl;
-        Xs[i] = (f < b.F && k < K) ? b.xe[(size_t)f * m.KTP + k] : 0.0f;
+        const int ai = f0 + fl;
+        Xs[i] = (ai < b.nact && k < K) ? b.xe[(size_t)b.act[ai] * m.KTP + k] : 0.0f;
     }
     __syncthreads();
     const int vl = threadIdx.x;
@@ -203,7 +204,27 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
 #pragma unroll
     for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
     const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
-    for (int k = 0; k < K; ++k) {
+    // sequential fused multiply-add over k for every output (the order the oracle uses)
+    int k = 0;
+    for (; k + 4 <= K; k += 4) {
+        float e[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) e[c][j] = Es[(c * KP + k + j) * 33 + vl];
+#pragma unroll
+        for (int q = 0; q < VT_FPT; ++q) {
+            const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
+            const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                acc[q][0] = fmaf(e[0][j], xv[j], acc[q][0]);
+                acc[q][1] = fmaf(e[1][j], xv[j], acc[q][1]);
+                acc[q][2] = fmaf(e[2][j], xv[j], acc[q][2]);
+            }
+        }
+    }
+    for (; k < K; ++k) {
         const float ex = Es[(0 * KP + k) * 33 + vl];
         const float ey = Es[(1 * KP + k) * 33 + vl];
         const float ez = Es[(2 * KP + k) * 33 + vl];
@@ -219,8 +240,10 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
     const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
 #pragma unroll
     for (int q = 0; q < VT_FPT; ++q) {
-        const int f = f0 + threadIdx.y * VT_FPT + q;
-        if (f >= b.F || !b.ctl[f].render) continue;
+        const int ai = f0 + threadIdx.y * VT_FPT + q;
+        if (ai >= b.nact) continue;
+        const int f = b.act[ai];
+        if (!b.ctl[f].render) continue;
         const float *R = b.R + f * 9;
         const float *tau = b.xe + (size_t)f * m.KTP + K;
         const float *cam = b.cam + f * 4;
@@ -232,9 +255,7 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
         g[v] = X0;
         g[m.V + v] = Y0;
         g[2 * m.V + v] = Z0;
-        g[3 * m.V + v] = (cam[0] * X3) / Z3 + cam[2];
-        g[4 * m.V + v] = (cam[1] * Y3) / Z3 + cam[3];
-        g[5 * m.V + v] = Z3;
+        b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
     }
 }
 
@@ -242,67 +263,78 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
 // Barrier objective of a state (logbarrier_initializer.cu:1921-2093 with compute_Gs :456-520):
 // expression bounds, then the four landmark box constraints. Landmark 3D points are the
 // vertex-stage object coordinates at the landmark vertices (same formula as the reference's
-// p0L + EL*eps). Sequential FP64 sum in the oracle's order.
+// p0L + EL*eps). One warp per frame: lanes evaluate the -log terms (FP64 log rounded to FP32),
+// lane 0 sums them sequentially in FP64 in the oracle's order.
 
-__device__ double barrier_objective(const DModel &m, const DBatch &b, int f, int ft_bounds,
-                                    float G[4][NL])
+__device__ __forceinline__ void landmark_G(const DModel &m, const DBatch &b, int f, const float *x,
+                                           const float *R, int i, float G[4])
 {
-    const float *x = b.xe + (size_t)f * m.KTP;
-    const float *R = b.R + f * 9;
     const float *tau = x + m.K;
     const float *geo = b.geo + (size_t)f * 6 * m.V;
-    const float *lb = m.eps_b + (ft_bounds ? 2 : 0) * m.K;
-    const float *ub = m.eps_b + (ft_bounds ? 3 : 1) * m.K;
     const float *cam = b.cam + f * 4;
-    const float phix = cam[0], phiy = cam[1], cx = cam[2], cy = cam[3];
     const float fs = b.face_size[f];
     const float *bnd = b.bounds + (size_t)f * 4 * NL;
-    const float *xl = b.xl + f * NL, *yl = b.yl + f * NL;
-    double obj = 0.0;
-    for (int k = 0; k < m.K; ++k) {
-        float fub = x[k] - ub[k];
-        float flb = lb[k] - x[k];
-        obj += (double)(-(float)log((double)(-flb)));
-        obj += (double)(-(float)log((double)(-fub)));
-    }
-    for (int i = 0; i < NL; ++i) {
-        const int v = m.lis[i];
-        const float p0 = geo[v], p1 = geo[m.V + v], p2 = geo[2 * m.V + v];
-        const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
-        const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
-        const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
-        const float xproj = phix * ((r1p + tau[0]) / (r3p + tau[2])) + cx;
-        const float yproj = phiy * ((r2p + tau[1]) / (r3p + tau[2])) + cy;
-        G[0][i] = 0.0f - ((xl[i] + bnd[0 * NL + i] * fs) - xproj);
-        G[1][i] = 0.0f - ((yl[i] + bnd[1 * NL + i] * fs) - yproj);
-        G[2][i] = 0.0f - ((xproj - bnd[2 * NL + i] * fs) - xl[i]);
-        G[3][i] = 0.0f - ((yproj - bnd[3 * NL + i] * fs) - yl[i]);
-    }
-    for (int s = 0; s < 4; ++s)
-        for (int i = 0; i < NL; ++i) obj += (double)(-(float)log((double)G[s][i]));
-    return obj;
+    const float xl = b.xl[f * NL + i], yl = b.yl[f * NL + i];
+    const int v = m.lis[i];
+    const float p0 = geo[v], p1 = geo[m.V + v], p2 = geo[2 * m.V + v];
+    const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
+    const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
+    const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
+    const float xproj = cam[0] * ((r1p + tau[0]) / (r3p + tau[2])) + cam[2];
+    const float yproj = cam[1] * ((r2p + tau[1]) / (r3p + tau[2])) + cam[3];
+    G[0] = 0.0f - ((xl + bnd[0 * NL + i] * fs) - xproj);
+    G[1] = 0.0f - ((yl + bnd[1 * NL + i] * fs) - yproj);
+    G[2] = 0.0f - ((xproj - bnd[2 * NL + i] * fs) - xl);
+    G[3] = 0.0f - ((yproj - bnd[3 * NL + i] * fs) - yl);
 }
 
 // Face-size check (renderer.cu:838-857), barrier objective and the pre-render decisions of
 // a trial (model_fitter.cu:237-300): tau_z, face size, NaN barrier, then -g.d < 3e-4.
-__global__ void k_precheck(DModel m, DBatch b, Cfg c, int stage)
+constexpr int PC_WARPS = 4;
+
+__global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, Cfg c, int stage)
 {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.F) return;
+    extern __shared__ float pterm[];             // [PC_WARPS][2K + 4*NL]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * PC_WARPS + warp;
+    if (i >= b.nact) return;
+    const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active || !ctl.render) return;
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
-    const float *xp = geo + 3 * m.V, *yp = geo + 4 * m.V;
+    const float4 *pj = b.proj + (size_t)f * m.V;
     const int *L = m.lis;
-    const float d_iod = fabsf(xp[L[9]] - xp[L[0]]);
-    const float d_lem = fabsf(yp[L[0]] - yp[L[40]]);
-    const float d_rem = fabsf(yp[L[9]] - yp[L[40]]);
+    const float d_iod = fabsf(pj[L[9]].x - pj[L[0]].x);
+    const float d_lem = fabsf(pj[L[0]].y - pj[L[40]].y);
+    const float d_rem = fabsf(pj[L[9]].y - pj[L[40]].y);
     const double lim = (double)c.ref_face_size * 2;
     const int face_ok = !((double)d_iod > lim || (double)d_lem > lim || (double)d_rem > lim);
+    if (!shape_stage(stage)) {
+        if (lane == 0) ctl.face_ok = face_ok;
+        return;
+    }
+    const int nterm = 2 * m.K + 4 * NL;
+    float *t = pterm + warp * nterm;
+    const float *x = b.xe + (size_t)f * m.KTP;
+    const float *R = b.R + f * 9;
+    const bool ft = stage == ST_FINETUNE;
+    const float *lb = m.eps_b + (ft ? 2 : 0) * m.K;
+    const float *ub = m.eps_b + (ft ? 3 : 1) * m.K;
+    for (int k = lane; k < m.K; k += 32) {
+        const float fub = x[k] - ub[k];
+        const float flb = lb[k] - x[k];
+        t[2 * k] = -(float)log((double)(-flb));
+        t[2 * k + 1] = -(float)log((double)(-fub));
+    }
+    for (int li = lane; li < NL; li += 32) {
+        float G[4];
+        landmark_G(m, b, f, x, R, li, G);
+        for (int sset = 0; sset < 4; ++sset) t[2 * m.K + sset * NL + li] = -(float)log((double)G[sset]);
+    }
+    __syncwarp();
+    if (lane != 0) return;
     ctl.face_ok = face_ok;
-    if (!shape_stage(stage)) return;
-    float G[4][NL];
-    const double ob = barrier_objective(m, b, f, stage == ST_FINETUNE, G);
+    double ob = 0.0;
+    for (int q = 0; q < nterm; ++q) ob += (double)t[q];
     ctl.obj_b = (float)ob;
     if (ctl.mode != M_TRIAL) return;
     if (!face_ok || isnan(ob)) {
@@ -326,14 +358,16 @@ __global__ void k_precheck(DModel m, DBatch b, Cfg c, int stage)
 // them in slot order (row-major over r, then triangle). The pixel owner is the minimum key
 // (smallest triangle among depth ties). Slot 0 is dropped, as remove_if(is_zero) does.
 
-__device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, const float *yp,
-                                             int idx, int x0, int y0, uint16_t pix[NTMP],
-                                             float al[NTMP], float be[NTMP], uint32_t &flags)
+template <class Fetch>
+__device__ __forceinline__ int tri_fragments_t(const DModel &m, Fetch fetch, int idx, int x0, int y0,
+                                               uint16_t pix[NTMP], float al[NTMP], float be[NTMP],
+                                               uint32_t &flags)
 {
     const int T = m.T;
     const int ib = m.tl[idx], ic = m.tl[T + idx], ia = m.tl[2 * T + idx];
-    const float bx = xp[ib], cx = xp[ic], ax = xp[ia];
-    const float by = yp[ib], cy = yp[ic], ay = yp[ia];
+    const float2 pb = fetch(ib), pc = fetch(ic), pa = fetch(ia);
+    const float bx = pb.x, cx = pc.x, ax = pa.x;
+    const float by = pb.y, cy = pc.y, ay = pa.y;
     const float xhi = ceilf(fmaxf(fmaxf(bx, cx), ax));
     const float yhi = ceilf(fmaxf(fmaxf(by, cy), ay));
     float xlo_f = floorf(fminf(fminf(bx, cx), ax));
@@ -350,22 +384,39 @@ __device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, c
         flags |= FLAG_OUT_OF_DOMAIN;
         return 0;
     }
-    const uint16_t xlo = (uint16_t)xlo_f, ylo = (uint16_t)ylo_f;
+    // The reference recomputes these per sample point; they do not depend on it.
+    const float v0x = bx - ax, v1x = cx - ax;
+    const float v0y = by - ay, v1y = cy - ay;
+    const float d00 = v0x * v0x + v0y * v0y;
+    const float d01 = v0x * v1x + v0y * v1y;
+    const float d11 = v1x * v1x + v1y * v1y;
+    const float denom = d00 * d11 - d01 * d01;
+    // With a zero or NaN denominator no sample can pass (alpha, beta become inf/NaN and
+    // alpha + beta <= 1 fails).
+    if (!(denom > 0.0f) && !(denom < 0.0f)) return 0;
+    const bool dpos = denom > 0.0f;
     int ridx = 0;
-    for (uint16_t x = xlo; (float)x < xhi && ridx < NTMP; ++x) {
-        for (uint16_t y = ylo; (float)y < yhi && ridx < NTMP; ++y) {
-            float v0x = bx - ax, v1x = cx - ax, v2x = (float)x - ax;
-            float v0y = by - ay, v1y = cy - ay, v2y = (float)y - ay;
-            float d00 = v0x * v0x + v0y * v0y;
-            float d01 = v0x * v1x + v0y * v1y;
-            float d11 = v1x * v1x + v1y * v1y;
-            float d20 = v0x * v2x + v0y * v2y;
-            float d21 = v1x * v2x + v1y * v2y;
-            float denom = d00 * d11 - d01 * d01;
-            float alpha = (d11 * d20 - d01 * d21) / denom;
-            float beta = (d00 * d21 - d01 * d20) / denom;
+    // Loop counters are kept as floats (integers below 2^24 are exact), which is what the
+    // reference's ushort counters are converted to in every comparison and subtraction.
+    int xi = (int)xlo_f;
+    for (float xf = xlo_f; xf < xhi && ridx < NTMP; xf += 1.0f, ++xi) {
+        const float v2x = xf - ax;
+        int yi = (int)ylo_f;
+        for (float yf = ylo_f; yf < yhi && ridx < NTMP; yf += 1.0f, ++yi) {
+            const float v2y = yf - ay;
+            const float d20 = v0x * v2x + v0y * v2y;
+            const float d21 = v1x * v2x + v1y * v2y;
+            // alpha = na/denom > 0 and beta = nb/denom > 0 need na, nb to have denom's sign
+            // (a quotient of opposite signs, of a zero or of a NaN is not > 0): samples that
+            // fail this skip the divisions; the rest take the exact test.
+            const float na = d11 * d20 - d01 * d21;
+            if (!(dpos ? na > 0.0f : na < 0.0f)) continue;
+            const float nb = d00 * d21 - d01 * d20;
+            if (!(dpos ? nb > 0.0f : nb < 0.0f)) continue;
+            const float alpha = na / denom;
+            const float beta = nb / denom;
             if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
-                int px = ((int)y - y0) + ((int)x - x0) * DIM;
+                int px = (yi - y0) + (xi - x0) * DIM;
                 if (px < 0 || px >= NPIX) flags |= FLAG_OUT_OF_DOMAIN;
                 pix[ridx] = (uint16_t)px;
                 al[ridx] = alpha;
@@ -375,6 +426,23 @@ __device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, c
         }
     }
     return ridx;
+}
+
+// projections as separate planes (caller-owned arrays)
+__device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, const float *yp,
+                                             int idx, int x0, int y0, uint16_t pix[NTMP],
+                                             float al[NTMP], float be[NTMP], uint32_t &flags)
+{
+    return tri_fragments_t(m, [&](int v) { return make_float2(xp[v], yp[v]); }, idx, x0, y0, pix, al, be, flags);
+}
+
+// projections packed per vertex (the batch's proj array)
+__device__ __forceinline__ int tri_fragments(const DModel &m, const float4 *pj, int idx, int x0, int y0,
+                                             uint16_t pix[NTMP], float al[NTMP], float be[NTMP],
+                                             uint32_t &flags)
+{
+    return tri_fragments_t(m, [&](int v) { const float4 q = __ldg(pj + v); return make_float2(q.x, q.y); },
+                           idx, x0, y0, pix, al, be, flags);
 }
 
 __device__ __forceinline__ unsigned long long zkey(uint32_t tag, float Z, int tri)
@@ -395,11 +463,27 @@ __device__ __forceinline__ bool survives(unsigned long long k, uint32_t tag, uin
     return (uint32_t)(k >> (31 + TRI_BITS)) == tag && (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zbits;
 }
 
+// Cluster-wide exclusive offset of this block's per-row totals s_blk (all blocks call it).
+__device__ __forceinline__ void cluster_offsets(cooperative_groups::cluster_group &cluster, int rank,
+                                                const uint32_t *s_blk, int nrows, uint32_t *blkoff,
+                                                uint32_t *total)
+{
+    for (int r = 0; r < nrows; ++r) { blkoff[r] = 0; total[r] = 0; }
+    for (int q = 0; q < RC; ++q) {
+        const uint32_t *rb = cluster.map_shared_rank(s_blk, q);
+        for (int r = 0; r < nrows; ++r) {
+            const uint32_t v = rb[r];
+            if (q == rank) blkoff[r] = total[r];
+            total[r] += v;
+        }
+    }
+}
+
 __global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DModel m, DBatch b)
 {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    const int f = blockIdx.x / RC;
+    const int f = b.act[blockIdx.x / RC];
     const int rank = (int)cluster.block_rank();
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.render) return;                 // the whole cluster belongs to this frame
@@ -410,8 +494,10 @@ __global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DMod
     __shared__ int s_bbox[4];
     __shared__ uint32_t s_flags;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
     unsigned long long *zb = b.zbuf + (size_t)f * NPIX;
     uint8_t *cnt8 = b.tri_cnt + (size_t)f * m.T;
+    int32_t *list = b.tri_list + (size_t)f * m.T;
     uint32_t epoch = ctl.epoch + 1;
     const bool wrap = epoch > TAG_MAX;
     if (wrap) epoch = 1;
@@ -425,26 +511,29 @@ __global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DMod
     __threadfence();
     cluster.sync();
     const uint32_t tag = TAG_MAX - epoch;
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
-    const float *xp = geo + 3 * m.V, *yp = geo + 4 * m.V, *Zc = geo + 5 * m.V;
+    const float4 *pj = b.proj + (size_t)f * m.V;
     const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
     const int T = m.T;
     const int gwarps = RC * RWARPS;
+    const int gw = rank * RWARPS + warp;
     const int per_warp = ((T + gwarps * 32 - 1) / (gwarps * 32)) * 32;
-    const int t_begin = (rank * RWARPS + warp) * per_warp;
+    const int t_begin = gw * per_warp;
     const int t_end = min(T, t_begin + per_warp);
     uint32_t flags = 0;
     int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
 
-    // pass A: depth keys, fragment count per triangle
+    // pass A: depth keys and the fragment count of each triangle. The z-buffer does not
+    // depend on the order, so triangles are visited in Morton order of their centroids:
+    // neighbouring lanes then gather neighbouring vertices.
     for (int base = t_begin; base < t_end; base += 32) {
-        const int idx = base + lane;
-        if (idx < t_end) {
+        const int slot = base + lane;
+        if (slot < t_end) {
+            const int idx = m.tri_order[slot];
             uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-            const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, flags);
+            const int nf = tri_fragments(m, pj, idx, x0, y0, pix, al, be, flags);
             cnt8[idx] = (uint8_t)nf;
             if (nf) {
-                const float Z = Zc[m.tl[idx]];
+                const float Z = pj[m.tl[idx]].z;
                 if (!(Z > 0.0f)) flags |= FLAG_OUT_OF_DOMAIN;
                 const unsigned long long key = zkey(tag, Z, idx);
                 for (int r = 0; r < nf; ++r) atomicMin(zb + pix[r], key);
@@ -454,43 +543,67 @@ __global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DMod
     __threadfence();
     cluster.sync();
 
-    // pass B: survivors per row, warp and block
-    uint32_t cnt[NTMP] = {0, 0, 0, 0};
-    for (int base = t_begin; base < t_end; base += 32) {
-        const int idx = base + lane;
-        bool sv[NTMP] = {false, false, false, false};
-        if (idx < t_end && cnt8[idx]) {
-            uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-            uint32_t fl2 = 0;
-            const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
-            const uint32_t zbits = __float_as_uint(Zc[m.tl[idx]]) & 0x7FFFFFFFu;
-            for (int r = 0; r < nf; ++r)
-                sv[r] = survives(__ldcg(zb + pix[r]), tag, zbits) && !(r == 0 && idx == 0);
-        }
-#pragma unroll
-        for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
-    }
-    if (lane == 0)
-        for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
-    __syncthreads();
-    if (tid < NTMP) {
-        uint32_t tot = 0;
-        for (int w = 0; w < RWARPS; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
-        s_blk[tid] = tot;
-    }
-    cluster.sync();
-    // frame totals per row and the offset of this block within each row
-    uint32_t rowbase[NTMP], blkoff[NTMP];
+    // list of the triangles that produced fragments, in ascending triangle order
     {
-        uint32_t tot[NTMP] = {0, 0, 0, 0};
-        for (int q = 0; q < RC; ++q) {
-            const uint32_t *rb = cluster.map_shared_rank(s_blk, q);
-            for (int r = 0; r < NTMP; ++r) {
-                const uint32_t v = rb[r];
-                if (q == rank) blkoff[r] = tot[r];
-                tot[r] += v;
-            }
+        uint32_t nz = 0;
+        for (int base = t_begin; base < t_end; base += 32) {
+            const int idx = base + lane;
+            nz += __popc(__ballot_sync(0xffffffffu, idx < t_end && cnt8[idx] != 0));
         }
+        if (lane == 0) s_cnt[warp][0] = nz;
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t tot = 0;
+            for (int w = 0; w < RWARPS; ++w) { s_off[w][0] = tot; tot += s_cnt[w][0]; }
+            s_blk[0] = tot;
+        }
+        cluster.sync();
+        uint32_t blkoff0, total0;
+        cluster_offsets(cluster, rank, s_blk, 1, &blkoff0, &total0);
+        uint32_t run = blkoff0 + s_off[warp][0];
+        for (int base = t_begin; base < t_end; base += 32) {
+            const int idx = base + lane;
+            const bool has = idx < t_end && cnt8[idx] != 0;
+            const unsigned mask = __ballot_sync(0xffffffffu, has);
+            if (has) list[run + __popc(mask & lt_mask)] = idx;
+            run += __popc(mask);
+        }
+        __threadfence();
+        cluster.sync();          // the list is complete; s_cnt/s_off/s_blk are free again
+        // entries of the list per warp, contiguous
+        const int L = (int)total0;
+        const int per_e = ((L + gwarps * 32 - 1) / (gwarps * 32)) * 32;
+        const int e_begin = gw * per_e;
+        const int e_end = min(L, e_begin + per_e);
+
+        // pass B: survivors per slot row, warp and block
+        uint32_t cnt[NTMP] = {0, 0, 0, 0};
+        for (int base = e_begin; base < e_end; base += 32) {
+            const int e = base + lane;
+            bool sv[NTMP] = {false, false, false, false};
+            if (e < e_end) {
+                const int idx = list[e];
+                uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
+                uint32_t fl2 = 0;
+                const int nf = tri_fragments(m, pj, idx, x0, y0, pix, al, be, fl2);
+                const uint32_t zbits = __float_as_uint(pj[m.tl[idx]].z) & 0x7FFFFFFFu;
+                for (int r = 0; r < nf; ++r)
+                    sv[r] = survives(__ldcg(zb + pix[r]), tag, zbits) && !(r == 0 && idx == 0);
+            }
+#pragma unroll
+            for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
+        }
+        if (lane == 0)
+            for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
+        __syncthreads();
+        if (tid < NTMP) {
+            uint32_t tot = 0;
+            for (int w = 0; w < RWARPS; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
+            s_blk[tid] = tot;
+        }
+        cluster.sync();
+        uint32_t rowbase[NTMP], blkoff[NTMP], tot[NTMP];
+        cluster_offsets(cluster, rank, s_blk, NTMP, blkoff, tot);
         uint32_t acc = 0;
         for (int r = 0; r < NTMP; ++r) { rowbase[r] = acc; acc += tot[r]; }
         if (tid == 0 && rank == 0) {
@@ -501,47 +614,48 @@ __global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DMod
             if (acc > 25600u) fl |= FLAG_OUT_OF_DOMAIN;
             atomicOr(&s_flags, fl);
         }
-    }
 
-    // pass C: write survivors in slot order
-    uint32_t run[NTMP] = {0, 0, 0, 0};
-    const unsigned lt_mask = (1u << lane) - 1u;
-    Fragment *out = b.frag + (size_t)f * NMAX;
-    for (int base = t_begin; base < t_end; base += 32) {
-        const int idx = base + lane;
-        bool sv[NTMP] = {false, false, false, false};
-        bool own[NTMP] = {false, false, false, false};
-        uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-        if (idx < t_end && cnt8[idx]) {
-            uint32_t fl2 = 0;
-            const int nf = tri_fragments(m, xp, yp, idx, x0, y0, pix, al, be, fl2);
-            const float Z = Zc[m.tl[idx]];
-            const uint32_t zbits = __float_as_uint(Z) & 0x7FFFFFFFu;
-            const unsigned long long mykey = zkey(tag, Z, idx);
-            for (int r = 0; r < nf; ++r) {
-                const unsigned long long k = __ldcg(zb + pix[r]);
-                sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
-                own[r] = (k == mykey);
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < NTMP; ++r) {
-            const unsigned mask = __ballot_sync(0xffffffffu, sv[r]);
-            if (sv[r]) {
-                const uint32_t pos = rowbase[r] + blkoff[r] + s_off[warp][r] + run[r] + __popc(mask & lt_mask);
-                if (pos < (uint32_t)NMAX) {
-                    Fragment fr;
-                    fr.pix_owner = (uint32_t)pix[r] | (own[r] ? 0x80000000u : 0u);
-                    fr.tri = idx;
-                    fr.al = al[r];
-                    fr.be = be[r];
-                    out[pos] = fr;
+        // pass C: write survivors in slot order (row, then triangle)
+        uint32_t run2[NTMP] = {0, 0, 0, 0};
+        Fragment *out = b.frag + (size_t)f * NMAX;
+        for (int base = e_begin; base < e_end; base += 32) {
+            const int e = base + lane;
+            bool sv[NTMP] = {false, false, false, false};
+            bool own[NTMP] = {false, false, false, false};
+            uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
+            int idx = -1;
+            if (e < e_end) {
+                idx = list[e];
+                uint32_t fl2 = 0;
+                const int nf = tri_fragments(m, pj, idx, x0, y0, pix, al, be, fl2);
+                const float Z = pj[m.tl[idx]].z;
+                const uint32_t zbits = __float_as_uint(Z) & 0x7FFFFFFFu;
+                const unsigned long long mykey = zkey(tag, Z, idx);
+                for (int r = 0; r < nf; ++r) {
+                    const unsigned long long k = __ldcg(zb + pix[r]);
+                    sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
+                    own[r] = (k == mykey);
                 }
-                const int px = pix[r] >> 8, py = pix[r] & 255;
-                bx0 = min(bx0, px); bx1 = max(bx1, px);
-                by0 = min(by0, py); by1 = max(by1, py);
             }
-            run[r] += __popc(mask);
+#pragma unroll
+            for (int r = 0; r < NTMP; ++r) {
+                const unsigned mask = __ballot_sync(0xffffffffu, sv[r]);
+                if (sv[r]) {
+                    const uint32_t pos = rowbase[r] + blkoff[r] + s_off[warp][r] + run2[r] + __popc(mask & lt_mask);
+                    if (pos < (uint32_t)NMAX) {
+                        Fragment fr;
+                        fr.pix_owner = (uint32_t)pix[r] | (own[r] ? 0x80000000u : 0u);
+                        fr.tri = idx;
+                        fr.al = al[r];
+                        fr.be = be[r];
+                        out[pos] = fr;
+                    }
+                    const int px = pix[r] >> 8, py = pix[r] & 255;
+                    bx0 = min(bx0, px); bx1 = max(bx1, px);
+                    by0 = min(by0, py); by1 = max(by1, py);
+                }
+                run2[r] += __popc(mask);
+            }
         }
     }
     if (flags) atomicOr(&s_flags, flags);
@@ -667,7 +781,7 @@ constexpr int RENDER_SMEM_FLOATS = 50 * 1024;   // two region buffers of up to 2
 
 __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, Cfg c, int stage)
 {
-    const int f = blockIdx.x;
+    const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.render) return;
     if (threadIdx.x == 0) prof_count(b, KID_RENDER);
@@ -754,8 +868,9 @@ __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, C
 // Shape fits (model_fitter.cu:215-356): objective -(tau*corr - barrier); Armijo test.
 __global__ void k_decide_shape(DModel m, DBatch b, Cfg c, int stage)
 {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.F) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b.nact) return;
+    const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active) return;
     const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
@@ -792,8 +907,9 @@ __global__ void k_decide_shape(DModel m, DBatch b, Cfg c, int stage)
 // Light fit (model_fitter.cu:981-1073): objective -corr; Armijo test with alpha = beta = 0.5.
 __global__ void k_decide_lambda(DModel m, DBatch b, Cfg c)
 {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.F) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b.nact) return;
+    const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active) return;
     if (ctl.flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) { ctl.active = 0; return; }
@@ -837,7 +953,7 @@ __device__ __forceinline__ uint32_t cnt_at(const uint32_t *cnt, int p)
 
 __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
 {
-    const int f = blockIdx.x;
+    const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!(all_frames ? ctl.render : ctl.need_jac)) return;
     if (threadIdx.x == 0) prof_count(b, KID_NEIGHBOURS);
@@ -962,7 +1078,7 @@ constexpr int JAC_WARPS = 8;
 
 __global__ void __launch_bounds__(JAC_WARPS * 32) k_jacobian(DModel m, DBatch b)
 {
-    const int f = blockIdx.y;
+    const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_JACOBIAN);
@@ -1070,7 +1186,7 @@ __host__ __device__ __forceinline__ int ne_part_stride(int KTP)
 // sum(w row), FP64, written to b.ne_part[f][split].
 __global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
 {
-    const int f = blockIdx.y, split = blockIdx.x;
+    const int f = b.act[blockIdx.y], split = blockIdx.x;
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (split == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
@@ -1145,7 +1261,7 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
 // Sum of the partial normal equations in split order: H = tau*S, g = -tau*w.
 __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatch b)
 {
-    const int f = blockIdx.x;
+    const int f = b.act[blockIdx.x];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     const int KTP = m.KTP, KT = m.KT, tid = threadIdx.x;
@@ -1181,7 +1297,7 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatc
 
 __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft_bounds)
 {
-    const int f = blockIdx.x;
+    const int f = b.act[blockIdx.x];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (threadIdx.x == 0) prof_count(b, KID_BARRIER);
@@ -1341,7 +1457,7 @@ __device__ int chol_solve_block(double *L, int n, const float *g, double *y)
 
 __global__ void __launch_bounds__(128) k_solve(DModel m, DBatch b, Cfg c, int stage)
 {
-    const int f = blockIdx.x;
+    const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (threadIdx.x == 0) prof_count(b, KID_SOLVE);
@@ -1384,7 +1500,7 @@ __global__ void __launch_bounds__(128) k_solve(DModel m, DBatch b, Cfg c, int st
 
 __global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
 {
-    const int f = blockIdx.x;
+    const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     __shared__ double s_red[8][12];
@@ -1505,17 +1621,35 @@ __global__ void k_paint(DModel m, DBatch b, float *images, int32_t *tri_map)
     }
 }
 
-// Frames still running the current stage.
-__global__ void k_count_active(DBatch b, int *out)
+// Frames still running the current stage, in ascending order (one block, block-wide scan).
+__global__ void __launch_bounds__(1024) k_compact_active(DBatch b, int *out)
 {
-    __shared__ int s;
-    if (threadIdx.x == 0) s = 0;
+    __shared__ int s_warp[32];
+    __shared__ int s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_base = 0;
     __syncthreads();
-    int c = 0;
-    for (int f = threadIdx.x; f < b.F; f += blockDim.x) c += b.ctl[f].active;
-    atomicAdd(&s, c);
-    __syncthreads();
-    if (threadIdx.x == 0) *out = s;
+    for (int f0 = 0; f0 < b.F; f0 += 1024) {
+        const int f = f0 + tid;
+        const int a = (f < b.F) ? b.ctl[f].active : 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, a);
+        if (lane == 0) s_warp[warp] = __popc(mask);
+        __syncthreads();
+        if (tid < 32) {
+            int v = s_warp[tid], incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (tid >= o) incl += t;
+            }
+            s_warp[tid] = incl - v;
+        }
+        __syncthreads();
+        if (a) b.act[s_base + s_warp[warp] + __popc(mask & ((1u << lane) - 1u))] = f;
+        __syncthreads();
+        if (tid == 1023) s_base += s_warp[31] + __popc(mask);
+        __syncthreads();
+    }
+    if (tid == 0) *out = s_base;
 }
 
 }  // namespace tdi
