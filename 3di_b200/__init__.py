@@ -96,7 +96,7 @@ SIGNATURES = {
 }
 
 KERNEL_IDS = dict(vertex=1, raster=2, render=3, neighbours=4, jacobian=5, normal_eq=6, barrier=7,
-                  solve=8)
+                  solve=8, raster_resolve=9)
 
 _lib = None
 

@@ -112,6 +112,7 @@ Cfg to_cfg(const tdi_fit_config &c)
 
 struct tdi_model {
     DModel d{};
+    std::vector<int32_t> vslot;    // internal slot of each vertex
     std::vector<void *> allocs;
     int device = 0;
 };
@@ -254,7 +255,8 @@ tdi_status geometry(const Launch &L, const Cfg &c, int stage)
     TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
                    (size_t)PC_WARPS * (2 * L.m.K + 4 * NL) * sizeof(float), L.s, L.m, L.b, c, stage));
-    TDI_TRY(launch(L.bt, KID_RASTER, k_raster, dim3(RC * L.A()), dim3(1024), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_RESOLVE, k_raster_resolve, dim3(L.A()), dim3(RR_THREADS), 0, L.s, L.m, L.b));
     return TDI_OK;
 }
 
@@ -353,61 +355,87 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
     DModel &d = m->d;
     d.V = V; d.T = T; d.K = K; d.KP = round4(K); d.KT = K + 6; d.KTP = round4(K + 6);
     float *mean, *E, *tex, *epsb;
-    int32_t *tl, *lis, *order;
+    int32_t *tl, *lis, *order, *tlo;
     auto cleanup = [&](tdi_status st) { for (void *p : m->allocs) cudaFree(p); delete m; return st; };
     tdi_status st;
     if ((st = dalloc(m->allocs, &mean, 3 * (size_t)V)) || (st = dalloc(m->allocs, &E, (size_t)V * 3 * d.KP)) ||
         (st = dalloc(m->allocs, &tex, (size_t)V)) || (st = dalloc(m->allocs, &tl, 3 * (size_t)T)) ||
         (st = dalloc(m->allocs, &lis, (size_t)NL)) || (st = dalloc(m->allocs, &epsb, 4 * (size_t)K)) ||
-        (st = dalloc(m->allocs, &order, (size_t)T)))
+        (st = dalloc(m->allocs, &order, (size_t)T)) || (st = dalloc(m->allocs, &tlo, 3 * (size_t)T)))
         return cleanup(st);
-    // Visiting order of the raster's depth pass: Morton order of the triangle centroids in
-    // the mean shape's x-y plane (the z-buffer result does not depend on the order).
-    std::vector<int32_t> tord(T);
+    // Internal vertex numbering: vertices are stored in Morton order of their mean-shape (x, y)
+    // position (slot), so that the corners of neighbouring triangles sit in neighbouring
+    // memory. Every per-vertex quantity is computed independently of the numbering; the
+    // entry points that take or return per-vertex arrays translate at the boundary.
+    // The raster's depth pass visits triangles in Morton order of their centroids (the
+    // z-buffer result does not depend on the order); tlo holds their corners as slots.
+    float xmin = desc->mean[0], xmax = xmin, ymin = desc->mean[V], ymax = ymin;
+    for (int v = 0; v < V; ++v) {
+        xmin = std::min(xmin, desc->mean[v]); xmax = std::max(xmax, desc->mean[v]);
+        ymin = std::min(ymin, desc->mean[V + v]); ymax = std::max(ymax, desc->mean[V + v]);
+    }
+    const float sx = 65535.0f / std::max(xmax - xmin, 1e-20f), sy = 65535.0f / std::max(ymax - ymin, 1e-20f);
+    auto spread = [](uint32_t x) {
+        x &= 0xFFFF;
+        x = (x | (x << 8)) & 0x00FF00FFu; x = (x | (x << 4)) & 0x0F0F0F0Fu;
+        x = (x | (x << 2)) & 0x33333333u; x = (x | (x << 1)) & 0x55555555u;
+        return x;
+    };
+    auto morton = [&](float x, float y) {
+        const uint32_t qx = (uint32_t)std::min(65535.0f, std::max(0.0f, (x - xmin) * sx));
+        const uint32_t qy = (uint32_t)std::min(65535.0f, std::max(0.0f, (y - ymin) * sy));
+        return spread(qx) | (spread(qy) << 1);
+    };
+    m->vslot.resize(V);
+    std::vector<int32_t> vord(V);
     {
-        float xmin = desc->mean[0], xmax = xmin, ymin = desc->mean[V], ymax = ymin;
-        for (int v = 0; v < V; ++v) {
-            xmin = std::min(xmin, desc->mean[v]); xmax = std::max(xmax, desc->mean[v]);
-            ymin = std::min(ymin, desc->mean[V + v]); ymax = std::max(ymax, desc->mean[V + v]);
-        }
+        std::vector<std::pair<uint32_t, int32_t>> keys(V);
+        for (int v = 0; v < V; ++v) keys[v] = {morton(desc->mean[v], desc->mean[V + v]), v};
+        std::sort(keys.begin(), keys.end());
+        for (int s = 0; s < V; ++s) { vord[s] = keys[s].second; m->vslot[keys[s].second] = s; }
+    }
+    std::vector<int32_t> tord(T), tls(3 * (size_t)T), tlo_h(3 * (size_t)T), lis_h(NL);
+    {
         std::vector<std::pair<uint32_t, int32_t>> keys(T);
-        auto spread = [](uint32_t x) {
-            x &= 0xFFFF;
-            x = (x | (x << 8)) & 0x00FF00FFu; x = (x | (x << 4)) & 0x0F0F0F0Fu;
-            x = (x | (x << 2)) & 0x33333333u; x = (x | (x << 1)) & 0x55555555u;
-            return x;
-        };
-        const float sx = 65535.0f / std::max(xmax - xmin, 1e-20f), sy = 65535.0f / std::max(ymax - ymin, 1e-20f);
         for (int t = 0; t < T; ++t) {
             float cx = 0.0f, cy = 0.0f;
             for (int r = 0; r < 3; ++r) {
                 const int v = desc->triangles[r * T + t];
                 cx += desc->mean[v]; cy += desc->mean[V + v];
             }
-            const uint32_t qx = (uint32_t)std::min(65535.0f, std::max(0.0f, (cx / 3.0f - xmin) * sx));
-            const uint32_t qy = (uint32_t)std::min(65535.0f, std::max(0.0f, (cy / 3.0f - ymin) * sy));
-            keys[t] = {spread(qx) | (spread(qy) << 1), t};
+            keys[t] = {morton(cx / 3.0f, cy / 3.0f), t};
         }
         std::sort(keys.begin(), keys.end());
         for (int t = 0; t < T; ++t) tord[t] = keys[t].second;
     }
+    for (int r = 0; r < 3; ++r)
+        for (int t = 0; t < T; ++t) tls[(size_t)r * T + t] = m->vslot[desc->triangles[(size_t)r * T + t]];
+    for (int r = 0; r < 3; ++r)
+        for (int s = 0; s < T; ++s) tlo_h[(size_t)r * T + s] = tls[(size_t)r * T + tord[s]];
+    for (int i = 0; i < NL; ++i) lis_h[i] = m->vslot[desc->landmarks[i]];
+    std::vector<float> mean_h(3 * (size_t)V), tex_h(V);
+    for (int c = 0; c < 3; ++c)
+        for (int s = 0; s < V; ++s) mean_h[(size_t)c * V + s] = desc->mean[(size_t)c * V + vord[s]];
+    for (int s = 0; s < V; ++s) tex_h[s] = desc->tex[vord[s]];
     std::vector<float> Ep((size_t)V * 3 * d.KP, 0.0f);
-    for (size_t r = 0; r < (size_t)V * 3; ++r)
-        std::memcpy(&Ep[r * d.KP], desc->expr_basis + r * K, sizeof(float) * K);
+    for (int s = 0; s < V; ++s)
+        for (int c = 0; c < 3; ++c)
+            std::memcpy(&Ep[((size_t)s * 3 + c) * d.KP], desc->expr_basis + ((size_t)vord[s] * 3 + c) * K, sizeof(float) * K);
     std::vector<float> eb(4 * (size_t)K);
     std::memcpy(&eb[0], desc->eps_lb, sizeof(float) * K);
     std::memcpy(&eb[K], desc->eps_ub, sizeof(float) * K);
     std::memcpy(&eb[2 * K], desc->eps_lb_finetune, sizeof(float) * K);
     std::memcpy(&eb[3 * K], desc->eps_ub_finetune, sizeof(float) * K);
-    if (cudaMemcpy(mean, desc->mean, sizeof(float) * 3 * V, cudaMemcpyHostToDevice) != cudaSuccess ||
+    if (cudaMemcpy(mean, mean_h.data(), sizeof(float) * 3 * V, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(E, Ep.data(), sizeof(float) * Ep.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(tex, desc->tex, sizeof(float) * V, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(tl, desc->triangles, sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(lis, desc->landmarks, sizeof(int32_t) * NL, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tex, tex_h.data(), sizeof(float) * V, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tl, tls.data(), sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(lis, lis_h.data(), sizeof(int32_t) * NL, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(epsb, eb.data(), sizeof(float) * eb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(order, tord.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(order, tord.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tlo, tlo_h.data(), sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess)
         return cleanup(fail(TDI_ERR_CUDA, "model upload failed"));
-    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb; d.tri_order = order;
+    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb; d.tri_order = order; d.tlo = tlo;
     *out = m;
     return TDI_OK;
 }
@@ -445,7 +473,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
-    A(d.ctl, F); A(d.act, F); A(d.geo, F * 6 * md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_cnt, F * (size_t)md.T); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
+    A(d.ctl, F); A(d.act, F); A(d.geo, F * 6 * md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
     A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_SPLIT * (size_t)ne_part_stride((int)KTP)); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
     A(d.prof_frames, 1);
@@ -454,6 +482,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     if (cudaMallocHost(&b->h_count, sizeof(int)) != cudaSuccess) return cleanup(fail(TDI_ERR_NOMEM, "pinned alloc"));
     if (cudaMemset(d.zbuf, 0xFF, F * NPIX * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemset(d.ctl, 0, F * sizeof(FrameCtl)) != cudaSuccess ||
+        cudaMemset(d.tri_mask, 0, F * mask_words(md.T) * sizeof(uint32_t)) != cudaSuccess ||
         cudaMemset(d.x, 0, F * KTP * sizeof(float)) != cudaSuccess ||
         cudaMemset(d.x_ls, 0, F * KTP * sizeof(float)) != cudaSuccess ||
         cudaMemset(d.J, 0, F * NMAX * KTP * sizeof(float)) != cudaSuccess ||
@@ -666,15 +695,23 @@ tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, 
         TDI_CUDA(cudaMemcpy(dst, b->scalars + (size_t)frame * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost));
         n = 4;
         break;
-    case 6:
+    case 6: {
         if (capacity < (int64_t)(6 * (size_t)m.V * sizeof(float))) return fail(TDI_ERR_INVALID, "destination too small");
-        TDI_CUDA(cudaMemcpy(dst, d.geo + (size_t)frame * 6 * m.V, 3 * (size_t)m.V * sizeof(float), cudaMemcpyDeviceToHost));
-        for (int c = 0; c < 3; ++c)
-            TDI_CUDA(cudaMemcpy2D(static_cast<float *>(dst) + (3 + c) * (size_t)m.V, sizeof(float),
-                                  reinterpret_cast<const float *>(d.proj + (size_t)frame * m.V) + c, sizeof(float4),
-                                  sizeof(float), m.V, cudaMemcpyDeviceToHost));
+        // stored by slot; returned in the caller's vertex numbering
+        std::vector<float> g(3 * (size_t)m.V);
+        std::vector<float4> pj(m.V);
+        TDI_CUDA(cudaMemcpy(g.data(), d.geo + (size_t)frame * 6 * m.V, 3 * (size_t)m.V * sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(pj.data(), d.proj + (size_t)frame * m.V, (size_t)m.V * sizeof(float4), cudaMemcpyDeviceToHost));
+        float *o = static_cast<float *>(dst);
+        const std::vector<int32_t> &vs = b->m->vslot;
+        for (int v = 0; v < m.V; ++v) {
+            const size_t sl = (size_t)vs[v];
+            o[v] = g[sl]; o[m.V + v] = g[m.V + sl]; o[2 * (size_t)m.V + v] = g[2 * (size_t)m.V + sl];
+            o[3 * (size_t)m.V + v] = pj[sl].x; o[4 * (size_t)m.V + v] = pj[sl].y; o[5 * (size_t)m.V + v] = pj[sl].z;
+        }
         n = 6 * (int64_t)m.V;
         break;
+    }
     default:
         return fail(TDI_ERR_INVALID, "unknown item");
     }
@@ -689,7 +726,7 @@ tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const 
     const DModel &m = b->m->d;
     DBatch &d = b->d;
     std::vector<float4> pj(m.V);
-    for (int v = 0; v < m.V; ++v) pj[v] = make_float4(xp[v], yp[v], zc[v], 0.0f);
+    for (int v = 0; v < m.V; ++v) pj[b->m->vslot[v]] = make_float4(xp[v], yp[v], zc[v], 0.0f);
     TDI_CUDA(cudaMemcpy(d.proj + (size_t)frame * m.V, pj.data(), sizeof(float4) * m.V, cudaMemcpyHostToDevice));
     int32_t o[2] = {x0, y0};
     TDI_CUDA(cudaMemcpy((void *)(d.x0y0 + 2 * frame), o, sizeof(o), cudaMemcpyHostToDevice));
@@ -698,7 +735,8 @@ tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const 
     TDI_CUDA(cudaMemcpy(d.act, &frame, sizeof(int32_t), cudaMemcpyHostToDevice));
     d.nact = 1;
     TDI_TRY(launch(b, 0, k_set_render, dim3(1), dim3(256), 0, (cudaStream_t)0, d, (int)frame));
-    TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC), dim3(1024), 0, (cudaStream_t)0, m, d));
+    TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, 1), dim3(RD_THREADS), 0, (cudaStream_t)0, m, d));
+    TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(1), dim3(RR_THREADS), 0, (cudaStream_t)0, m, d));
     TDI_CUDA(cudaDeviceSynchronize());
     FrameCtl ctl;
     TDI_CUDA(cudaMemcpy(&ctl, d.ctl + frame, sizeof(FrameCtl), cudaMemcpyDeviceToHost));
@@ -725,7 +763,8 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
         TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
         dim3 vg((m.V + VT_V - 1) / VT_V, (n + VT_F - 1) / VT_F);
         TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
-        TDI_TRY(launch(b, KID_RASTER, k_raster, dim3(RC * n), dim3(1024), 0, s, m, d));
+        TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, n), dim3(RD_THREADS), 0, s, m, d));
+        TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));
     }
     float *img = d.img;                                   // [F][NPIX] image, then [F][NPIX] map
     int32_t *map = reinterpret_cast<int32_t *>(d.img + (size_t)d.F * NPIX);
@@ -745,7 +784,7 @@ tdi_status tdi_batch_launches(tdi_batch *b, int64_t *launches)
 
 tdi_status tdi_batch_profile(tdi_batch *b, int32_t kernel_id)
 {
-    if (!b || kernel_id < 0 || kernel_id > KID_SOLVE) return fail(TDI_ERR_INVALID, "bad kernel id");
+    if (!b || kernel_id < 0 || kernel_id > KID_RESOLVE) return fail(TDI_ERR_INVALID, "bad kernel id");
     for (auto &e : b->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     b->prof_events.clear();
     b->prof_id = kernel_id;

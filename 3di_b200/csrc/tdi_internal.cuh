@@ -23,6 +23,9 @@ constexpr int TRI_BITS = 20;      // z-buffer key: [13-bit epoch tag | 31-bit de
 constexpr int TAG_BITS = 64 - 31 - TRI_BITS;
 constexpr uint32_t TAG_MAX = (1u << TAG_BITS) - 1;
 
+// words of a per-frame bit set over the triangles
+__host__ __device__ constexpr inline int mask_words(int T) { return (T + 31) / 32; }
+
 // frame status bits (same values as the oracle and include/tdi.h)
 constexpr uint32_t FLAG_RENDER_SKIPPED = 1u;
 constexpr uint32_t FLAG_OUT_OF_DOMAIN = 2u;
@@ -74,16 +77,19 @@ struct Cfg {
 };
 
 // Device view of the model.
+// Vertices are numbered internally by slot (Morton order of the mean shape's x-y position);
+// tl and lis hold slots. Triangles keep the caller's numbering.
 struct DModel {
     int32_t V, T, K, KP;     // KP: K rounded up to a multiple of 4 (row pitch of E)
     int32_t KT, KTP;         // K + 6 unknowns, and its pitch (multiple of 4)
     const float *mean;       // [3][V]
     const float *E;          // [V][3][KP]
     const float *tex;        // [V]
-    const int32_t *tl;       // [3][T]
-    const int32_t *lis;      // [NL]
+    const int32_t *tl;       // [3][T] corner slots
+    const int32_t *lis;      // [NL] landmark slots
     const float *eps_b;      // [4][K]: lb, ub, lb_ft, ub_ft
     const int32_t *tri_order;// [T] triangles in Morton order of their mean-shape centroids
+    const int32_t *tlo;      // [3][T] corner slots of the triangles in tri_order
 };
 
 // Device view of a batch of frames and its working set.
@@ -110,7 +116,7 @@ struct DBatch {
     float *geo;              // [F][6][V]: X0, Y0, Z0 planes (planes 3-5 unused)
     float4 *proj;            // [F][V]: xp, yp, camera Z, 0 -- what the raster gathers
     unsigned long long *zbuf;// [F][NPIX]
-    uint8_t *tri_cnt;        // [F][T] fragments of each triangle in the last raster
+    uint32_t *tri_mask;      // [F][ceil(T/32)] triangles with fragments in the raster in flight
     int32_t *tri_list;       // [F][T] triangles with fragments, ascending
     Fragment *frag;          // [F][NMAX]
     float *fgrad;            // [F][5][NMAX]: gx, gy, h, gxs_n, gys_n

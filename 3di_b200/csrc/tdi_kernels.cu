@@ -71,7 +71,8 @@ __device__ void rotation(const float *u, float *R, float *dR)
 
 // Kernel ids for live profiling (tdi_batch_profile).
 enum KernelId : int32_t { KID_VERTEX = 1, KID_RASTER = 2, KID_RENDER = 3, KID_NEIGHBOURS = 4,
-                          KID_JACOBIAN = 5, KID_NORMAL_EQ = 6, KID_BARRIER = 7, KID_SOLVE = 8 };
+                          KID_JACOBIAN = 5, KID_NORMAL_EQ = 6, KID_BARRIER = 7, KID_SOLVE = 8,
+                          KID_RESOLVE = 9 };
 
 __device__ __forceinline__ void prof_count(const DBatch &b, int id, unsigned long long n = 1)
 {
@@ -350,24 +351,30 @@ __global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, 
 }
 
 // ------------------------------------------------------------------------------------------
-// Visibility: one 1024-thread block per frame (get_pixels_to_render + keep_only_minZ +
-// remove_if, funcs.cu:900-1029, renderer.cu:650-680). Pass A enumerates each triangle's
-// <= 4 fragments in bounding-box order and folds a 64-bit key
-// [epoch tag | depth bits | triangle id] into the frame's z-buffer with atomicMin; pass B
-// counts survivors (depth equal to the pixel minimum) per slot row and warp; pass C writes
-// them in slot order (row-major over r, then triangle). The pixel owner is the minimum key
-// (smallest triangle among depth ties). Slot 0 is dropped, as remove_if(is_zero) does.
+// Visibility (get_pixels_to_render + keep_only_minZ + remove_if, funcs.cu:900-1029,
+// renderer.cu:650-680) in two kernels.
+//
+// k_raster_depth: every triangle enumerates its <= 4 fragments in bounding-box order and
+// folds a 64-bit key [epoch tag | depth bits | triangle id] into the frame's z-buffer with
+// atomicMin; triangles with fragments set their bit in the frame's triangle mask. The
+// z-buffer does not depend on the visiting order, so triangles are visited in Morton order
+// of their centroids and their corners (vertex slots) lie close in memory.
+//
+// k_raster_resolve, one block per frame: lists the masked triangles in ascending order
+// (clearing the mask), counts the survivors of every slot row (depth equal to the pixel
+// minimum), and writes them in slot order (row r, then triangle). The pixel owner is the
+// minimum key (smallest triangle among depth ties). Slot 0 is dropped, as remove_if(is_zero)
+// does. The epoch tag makes earlier renders' keys lose to this one's without clearing the
+// z-buffer; it is cleared once the tag range is used up.
 
-template <class Fetch>
-__device__ __forceinline__ int tri_fragments_t(const DModel &m, Fetch fetch, int idx, int x0, int y0,
-                                               uint16_t pix[NTMP], float al[NTMP], float be[NTMP],
-                                               uint32_t &flags)
+// Samples of one triangle with corners b, c, a (rows 0, 1, 2 of the triangle list) in the
+// reference's order: x-major over the integer points of the bounding box, at most NTMP.
+// emit(r, pix, alpha, beta) receives each, pix wrapped to 16 bits as the reference's
+// ushort index is; the count is returned.
+template <class Emit>
+__device__ __forceinline__ int tri_samples(float bx, float by, float cx, float cy, float ax, float ay,
+                                           int x0, int y0, uint32_t &flags, Emit &&emit)
 {
-    const int T = m.T;
-    const int ib = m.tl[idx], ic = m.tl[T + idx], ia = m.tl[2 * T + idx];
-    const float2 pb = fetch(ib), pc = fetch(ic), pa = fetch(ia);
-    const float bx = pb.x, cx = pc.x, ax = pa.x;
-    const float by = pb.y, cy = pc.y, ay = pa.y;
     const float xhi = ceilf(fmaxf(fmaxf(bx, cx), ax));
     const float yhi = ceilf(fmaxf(fmaxf(by, cy), ay));
     float xlo_f = floorf(fminf(fminf(bx, cx), ax));
@@ -416,16 +423,26 @@ __device__ __forceinline__ int tri_fragments_t(const DModel &m, Fetch fetch, int
             const float alpha = na / denom;
             const float beta = nb / denom;
             if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
-                int px = (yi - y0) + (xi - x0) * DIM;
+                const int px = (yi - y0) + (xi - x0) * DIM;
                 if (px < 0 || px >= NPIX) flags |= FLAG_OUT_OF_DOMAIN;
-                pix[ridx] = (uint16_t)px;
-                al[ridx] = alpha;
-                be[ridx] = beta;
+                emit(ridx, (uint32_t)(uint16_t)px, alpha, beta);
                 ridx++;
             }
         }
     }
     return ridx;
+}
+
+// Fragments of triangle idx into arrays, corners fetched through fetch(v) -> float2.
+template <class Fetch>
+__device__ __forceinline__ int tri_fragments_t(const DModel &m, Fetch fetch, int idx, int x0, int y0,
+                                               uint16_t pix[NTMP], float al[NTMP], float be[NTMP],
+                                               uint32_t &flags)
+{
+    const int T = m.T;
+    const float2 pb = fetch(m.tl[idx]), pc = fetch(m.tl[T + idx]), pa = fetch(m.tl[2 * T + idx]);
+    return tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, flags,
+                       [&](int r, uint32_t px, float a, float b) { pix[r] = (uint16_t)px; al[r] = a; be[r] = b; });
 }
 
 // projections as separate planes (caller-owned arrays)
@@ -436,15 +453,6 @@ __device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, c
     return tri_fragments_t(m, [&](int v) { return make_float2(xp[v], yp[v]); }, idx, x0, y0, pix, al, be, flags);
 }
 
-// projections packed per vertex (the batch's proj array)
-__device__ __forceinline__ int tri_fragments(const DModel &m, const float4 *pj, int idx, int x0, int y0,
-                                             uint16_t pix[NTMP], float al[NTMP], float be[NTMP],
-                                             uint32_t &flags)
-{
-    return tri_fragments_t(m, [&](int v) { const float4 q = __ldg(pj + v); return make_float2(q.x, q.y); },
-                           idx, x0, y0, pix, al, be, flags);
-}
-
 __device__ __forceinline__ unsigned long long zkey(uint32_t tag, float Z, int tri)
 {
     return ((unsigned long long)tag << (31 + TRI_BITS)) |
@@ -452,236 +460,249 @@ __device__ __forceinline__ unsigned long long zkey(uint32_t tag, float Z, int tr
            (unsigned long long)(uint32_t)tri;
 }
 
-// One thread-block cluster of RC blocks per frame. Warps own consecutive ranges of
-// triangles (lanes take consecutive triangles), so slot order is warp order within a block,
-// block rank order within the cluster, and row r order across the frame.
-constexpr int RC = 8;                       // blocks per frame (cluster size)
-constexpr int RWARPS = 32;                  // warps per block
-
 __device__ __forceinline__ bool survives(unsigned long long k, uint32_t tag, uint32_t zbits)
 {
     return (uint32_t)(k >> (31 + TRI_BITS)) == tag && (uint32_t)((k >> TRI_BITS) & 0x7FFFFFFFu) == zbits;
 }
 
-// Cluster-wide exclusive offset of this block's per-row totals s_blk (all blocks call it).
-__device__ __forceinline__ void cluster_offsets(cooperative_groups::cluster_group &cluster, int rank,
-                                                const uint32_t *s_blk, int nrows, uint32_t *blkoff,
-                                                uint32_t *total)
+constexpr int RD_THREADS = 256;             // depth pass: threads per block
+constexpr int RD_BLOCKS = 16;               // depth pass: blocks per frame
+constexpr int RR_THREADS = 1024;            // resolve: one block per frame
+constexpr int RR_WARPS = RR_THREADS / 32;
+
+__global__ void __launch_bounds__(RD_THREADS) k_raster_depth(DModel m, DBatch b)
 {
-    for (int r = 0; r < nrows; ++r) { blkoff[r] = 0; total[r] = 0; }
-    for (int q = 0; q < RC; ++q) {
-        const uint32_t *rb = cluster.map_shared_rank(s_blk, q);
-        for (int r = 0; r < nrows; ++r) {
-            const uint32_t v = rb[r];
-            if (q == rank) blkoff[r] = total[r];
-            total[r] += v;
+    const int f = b.act[blockIdx.y];
+    const FrameCtl &ctl = b.ctl[f];
+    if (!ctl.render) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_RASTER);
+    const uint32_t tag = TAG_MAX - (ctl.epoch + 1);
+    const float4 *pj = b.proj + (size_t)f * m.V;
+    unsigned long long *zb = b.zbuf + (size_t)f * NPIX;
+    uint32_t *mask = b.tri_mask + (size_t)f * mask_words(m.T);
+    const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
+    const int T = m.T;
+    // each block a contiguous range of the Morton order
+    const int per_block = (T + RD_BLOCKS - 1) / RD_BLOCKS;
+    const int s_begin = blockIdx.x * per_block, s_end = min(T, s_begin + per_block);
+    uint32_t flags = 0;
+    for (int s = s_begin + (int)threadIdx.x; s < s_end; s += RD_THREADS) {
+        const int idx = __ldg(m.tri_order + s);
+        const float4 pb = __ldg(pj + __ldg(m.tlo + s));
+        const float4 pc = __ldg(pj + __ldg(m.tlo + T + s));
+        const float4 pa = __ldg(pj + __ldg(m.tlo + 2 * T + s));
+        const unsigned long long key = zkey(tag, pb.z, idx);
+        const int nf = tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, flags,
+                                   [&](int, uint32_t px, float, float) { atomicMin(zb + px, key); });
+        if (nf) {
+            if (!(pb.z > 0.0f)) flags |= FLAG_OUT_OF_DOMAIN;
+            atomicOr(mask + (idx >> 5), 1u << (idx & 31));
         }
     }
+    if (flags) atomicOr(&b.ctl[f].flags, flags);
 }
 
-__global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024) k_raster(DModel m, DBatch b)
+// Block-wide exclusive scan of one value per thread (RR_THREADS threads); returns the
+// thread's offset and writes the total to *total. Uses s_w[RR_WARPS].
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t *s_w, uint32_t *total)
 {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
-    const int f = b.act[blockIdx.x / RC];
-    const int rank = (int)cluster.block_rank();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = lane < RR_WARPS ? s_w[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < RR_WARPS) s_w[lane] = wi - w;
+        if (lane == 31) s_w[RR_WARPS] = wi;
+    }
+    __syncthreads();
+    const uint32_t off = s_w[warp] + inc - v;
+    *total = s_w[RR_WARPS];
+    __syncthreads();
+    return off;
+}
+
+__global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch b)
+{
+    const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
-    if (!ctl.render) return;                 // the whole cluster belongs to this frame
-    if (threadIdx.x == 0 && rank == 0) prof_count(b, KID_RASTER);
-    __shared__ uint32_t s_cnt[RWARPS][NTMP];   // survivors per warp and row
-    __shared__ uint32_t s_off[RWARPS][NTMP];   // exclusive offsets within the block
-    __shared__ uint32_t s_blk[NTMP];           // this block's totals per row (read by the cluster)
+    if (!ctl.render) return;
+    if (threadIdx.x == 0) prof_count(b, KID_RESOLVE);
+    __shared__ uint32_t s_w[RR_WARPS + 1];
+    __shared__ uint32_t s_cnt[RR_WARPS][NTMP];   // survivors per warp and row
+    __shared__ uint32_t s_off[RR_WARPS][NTMP];   // exclusive offsets of the warps per row
+    __shared__ uint32_t s_row[NTMP + 1];         // row bases; s_row[NTMP] = total
     __shared__ int s_bbox[4];
     __shared__ uint32_t s_flags;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
+    const int T = m.T;
+    const uint32_t epoch = ctl.epoch + 1;
+    const uint32_t tag = TAG_MAX - epoch;
     unsigned long long *zb = b.zbuf + (size_t)f * NPIX;
-    uint8_t *cnt8 = b.tri_cnt + (size_t)f * m.T;
-    int32_t *list = b.tri_list + (size_t)f * m.T;
-    uint32_t epoch = ctl.epoch + 1;
-    const bool wrap = epoch > TAG_MAX;
-    if (wrap) epoch = 1;
+    uint32_t *mask = b.tri_mask + (size_t)f * mask_words(T);
+    int32_t *list = b.tri_list + (size_t)f * T;
+    const float4 *pj = b.proj + (size_t)f * m.V;
+    const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
     if (tid == 0) {
         s_flags = 0;
         s_bbox[0] = s_bbox[2] = 1 << 30;
         s_bbox[1] = s_bbox[3] = -1;
     }
-    if (wrap)
-        for (int p = rank * 1024 + tid; p < NPIX; p += RC * 1024) zb[p] = ~0ull;
-    __threadfence();
-    cluster.sync();
-    const uint32_t tag = TAG_MAX - epoch;
-    const float4 *pj = b.proj + (size_t)f * m.V;
-    const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
-    const int T = m.T;
-    const int gwarps = RC * RWARPS;
-    const int gw = rank * RWARPS + warp;
-    const int per_warp = ((T + gwarps * 32 - 1) / (gwarps * 32)) * 32;
-    const int t_begin = gw * per_warp;
-    const int t_end = min(T, t_begin + per_warp);
-    uint32_t flags = 0;
-    int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
 
-    // pass A: depth keys and the fragment count of each triangle. The z-buffer does not
-    // depend on the order, so triangles are visited in Morton order of their centroids:
-    // neighbouring lanes then gather neighbouring vertices.
-    for (int base = t_begin; base < t_end; base += 32) {
-        const int slot = base + lane;
-        if (slot < t_end) {
-            const int idx = m.tri_order[slot];
-            uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-            const int nf = tri_fragments(m, pj, idx, x0, y0, pix, al, be, flags);
-            cnt8[idx] = (uint8_t)nf;
-            if (nf) {
-                const float Z = pj[m.tl[idx]].z;
-                if (!(Z > 0.0f)) flags |= FLAG_OUT_OF_DOMAIN;
-                const unsigned long long key = zkey(tag, Z, idx);
-                for (int r = 0; r < nf; ++r) atomicMin(zb + pix[r], key);
-            }
+    // list of the masked triangles, ascending: each thread a contiguous run of mask words
+    const int W = mask_words(T);
+    const int wpt = (W + RR_THREADS - 1) / RR_THREADS;
+    const int w_begin = min(W, tid * wpt), w_end = min(W, w_begin + wpt);
+    uint32_t nz = 0;
+    for (int w = w_begin; w < w_end; ++w) nz += __popc(__ldcg(mask + w));
+    uint32_t L;
+    uint32_t pos = block_scan(nz, s_w, &L);
+    for (int w = w_begin; w < w_end; ++w) {
+        uint32_t bits = __ldcg(mask + w);
+        if (bits) mask[w] = 0u;
+        while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1u;
+            list[pos++] = w * 32 + bit;
         }
     }
-    __threadfence();
-    cluster.sync();
+    __syncthreads();
+    // list entries per warp, contiguous; lanes take consecutive entries
+    const int per_e = (int)(((L + RR_WARPS * 32 - 1) / (RR_WARPS * 32)) * 32);
+    const int e_begin = min((int)L, warp * per_e);
+    const int e_end = min((int)L, e_begin + per_e);
 
-    // list of the triangles that produced fragments, in ascending triangle order
-    {
-        uint32_t nz = 0;
-        for (int base = t_begin; base < t_end; base += 32) {
-            const int idx = base + lane;
-            nz += __popc(__ballot_sync(0xffffffffu, idx < t_end && cnt8[idx] != 0));
+    // survivors per slot row and warp
+    uint32_t cnt[NTMP] = {0, 0, 0, 0};
+    for (int base = e_begin; base < e_end; base += 32) {
+        const int e = base + lane;
+        bool sv[NTMP] = {false, false, false, false};
+        if (e < e_end) {
+            const int idx = __ldcg(list + e);
+            const float4 pb = __ldg(pj + __ldg(m.tl + idx));
+            const float4 pc = __ldg(pj + __ldg(m.tl + T + idx));
+            const float4 pa = __ldg(pj + __ldg(m.tl + 2 * T + idx));
+            const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
+            uint32_t fl2 = 0;
+            tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, fl2, [&](int r, uint32_t px, float, float) {
+                sv[r] = survives(__ldcg(zb + px), tag, zbits) && !(r == 0 && idx == 0);
+            });
         }
-        if (lane == 0) s_cnt[warp][0] = nz;
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t tot = 0;
-            for (int w = 0; w < RWARPS; ++w) { s_off[w][0] = tot; tot += s_cnt[w][0]; }
-            s_blk[0] = tot;
-        }
-        cluster.sync();
-        uint32_t blkoff0, total0;
-        cluster_offsets(cluster, rank, s_blk, 1, &blkoff0, &total0);
-        uint32_t run = blkoff0 + s_off[warp][0];
-        for (int base = t_begin; base < t_end; base += 32) {
-            const int idx = base + lane;
-            const bool has = idx < t_end && cnt8[idx] != 0;
-            const unsigned mask = __ballot_sync(0xffffffffu, has);
-            if (has) list[run + __popc(mask & lt_mask)] = idx;
-            run += __popc(mask);
-        }
-        __threadfence();
-        cluster.sync();          // the list is complete; s_cnt/s_off/s_blk are free again
-        // entries of the list per warp, contiguous
-        const int L = (int)total0;
-        const int per_e = ((L + gwarps * 32 - 1) / (gwarps * 32)) * 32;
-        const int e_begin = gw * per_e;
-        const int e_end = min(L, e_begin + per_e);
-
-        // pass B: survivors per slot row, warp and block
-        uint32_t cnt[NTMP] = {0, 0, 0, 0};
-        for (int base = e_begin; base < e_end; base += 32) {
-            const int e = base + lane;
-            bool sv[NTMP] = {false, false, false, false};
-            if (e < e_end) {
-                const int idx = list[e];
-                uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-                uint32_t fl2 = 0;
-                const int nf = tri_fragments(m, pj, idx, x0, y0, pix, al, be, fl2);
-                const uint32_t zbits = __float_as_uint(pj[m.tl[idx]].z) & 0x7FFFFFFFu;
-                for (int r = 0; r < nf; ++r)
-                    sv[r] = survives(__ldcg(zb + pix[r]), tag, zbits) && !(r == 0 && idx == 0);
-            }
 #pragma unroll
-            for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
+        for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
+    }
+    if (lane == 0)
+        for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
+    __syncthreads();
+    if (warp == 0) {
+        // per row: exclusive scan over the warps (lane = warp index)
+        uint32_t rowsum[NTMP];
+#pragma unroll
+        for (int r = 0; r < NTMP; ++r) {
+            const uint32_t v = lane < RR_WARPS ? s_cnt[lane][r] : 0u;
+            uint32_t inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            if (lane < RR_WARPS) s_off[lane][r] = inc - v;
+            rowsum[r] = __shfl_sync(0xffffffffu, inc, 31);
         }
-        if (lane == 0)
-            for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
-        __syncthreads();
-        if (tid < NTMP) {
-            uint32_t tot = 0;
-            for (int w = 0; w < RWARPS; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
-            s_blk[tid] = tot;
-        }
-        cluster.sync();
-        uint32_t rowbase[NTMP], blkoff[NTMP], tot[NTMP];
-        cluster_offsets(cluster, rank, s_blk, NTMP, blkoff, tot);
-        uint32_t acc = 0;
-        for (int r = 0; r < NTMP; ++r) { rowbase[r] = acc; acc += tot[r]; }
-        if (tid == 0 && rank == 0) {
+        if (lane == 0) {
+            uint32_t acc = 0;
+            for (int r = 0; r < NTMP; ++r) { s_row[r] = acc; acc += rowsum[r]; }
+            s_row[NTMP] = acc;
             ctl.N = (int)min(acc, (uint32_t)NMAX);
             uint32_t fl = 0;
             if (acc > (uint32_t)NMAX) fl |= FLAG_OVERFLOW;
             if (acc < 1000u || acc > 52000u) fl |= FLAG_RENDER_SKIPPED;
             if (acc > 25600u) fl |= FLAG_OUT_OF_DOMAIN;
-            atomicOr(&s_flags, fl);
-        }
-
-        // pass C: write survivors in slot order (row, then triangle)
-        uint32_t run2[NTMP] = {0, 0, 0, 0};
-        Fragment *out = b.frag + (size_t)f * NMAX;
-        for (int base = e_begin; base < e_end; base += 32) {
-            const int e = base + lane;
-            bool sv[NTMP] = {false, false, false, false};
-            bool own[NTMP] = {false, false, false, false};
-            uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-            int idx = -1;
-            if (e < e_end) {
-                idx = list[e];
-                uint32_t fl2 = 0;
-                const int nf = tri_fragments(m, pj, idx, x0, y0, pix, al, be, fl2);
-                const float Z = pj[m.tl[idx]].z;
-                const uint32_t zbits = __float_as_uint(Z) & 0x7FFFFFFFu;
-                const unsigned long long mykey = zkey(tag, Z, idx);
-                for (int r = 0; r < nf; ++r) {
-                    const unsigned long long k = __ldcg(zb + pix[r]);
-                    sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
-                    own[r] = (k == mykey);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < NTMP; ++r) {
-                const unsigned mask = __ballot_sync(0xffffffffu, sv[r]);
-                if (sv[r]) {
-                    const uint32_t pos = rowbase[r] + blkoff[r] + s_off[warp][r] + run2[r] + __popc(mask & lt_mask);
-                    if (pos < (uint32_t)NMAX) {
-                        Fragment fr;
-                        fr.pix_owner = (uint32_t)pix[r] | (own[r] ? 0x80000000u : 0u);
-                        fr.tri = idx;
-                        fr.al = al[r];
-                        fr.be = be[r];
-                        out[pos] = fr;
-                    }
-                    const int px = pix[r] >> 8, py = pix[r] & 255;
-                    bx0 = min(bx0, px); bx1 = max(bx1, px);
-                    by0 = min(by0, py); by1 = max(by1, py);
-                }
-                run2[r] += __popc(mask);
-            }
+            s_flags = fl;
         }
     }
-    if (flags) atomicOr(&s_flags, flags);
+    __syncthreads();
+
+    // write survivors in slot order (row, then triangle)
+    uint32_t run[NTMP] = {0, 0, 0, 0};
+    uint32_t wbase[NTMP];
+#pragma unroll
+    for (int r = 0; r < NTMP; ++r) wbase[r] = s_row[r] + s_off[warp][r];
+    Fragment *out = b.frag + (size_t)f * NMAX;
+    int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
+    for (int base = e_begin; base < e_end; base += 32) {
+        const int e = base + lane;
+        bool sv[NTMP] = {false, false, false, false};
+        bool own[NTMP] = {false, false, false, false};
+        uint32_t pix[NTMP] = {0, 0, 0, 0};
+        float al[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f}, be[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f};
+        int idx = -1;
+        if (e < e_end) {
+            idx = __ldcg(list + e);
+            const float4 pb = __ldg(pj + __ldg(m.tl + idx));
+            const float4 pc = __ldg(pj + __ldg(m.tl + T + idx));
+            const float4 pa = __ldg(pj + __ldg(m.tl + 2 * T + idx));
+            const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
+            const unsigned long long mykey = zkey(tag, pb.z, idx);
+            uint32_t fl2 = 0;
+            tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, fl2, [&](int r, uint32_t px, float a, float bb) {
+                const unsigned long long k = __ldcg(zb + px);
+                sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
+                own[r] = (k == mykey);
+                pix[r] = px; al[r] = a; be[r] = bb;
+            });
+        }
+#pragma unroll
+        for (int r = 0; r < NTMP; ++r) {
+            const unsigned msk = __ballot_sync(0xffffffffu, sv[r]);
+            if (sv[r]) {
+                const uint32_t p = wbase[r] + run[r] + __popc(msk & lt_mask);
+                if (p < (uint32_t)NMAX) {
+                    Fragment fr;
+                    fr.pix_owner = pix[r] | (own[r] ? 0x80000000u : 0u);
+                    fr.tri = idx;
+                    fr.al = al[r];
+                    fr.be = be[r];
+                    out[p] = fr;
+                }
+                const int px = (int)(pix[r] >> 8), py = (int)(pix[r] & 255);
+                bx0 = min(bx0, px); bx1 = max(bx1, px);
+                by0 = min(by0, py); by1 = max(by1, py);
+            }
+            run[r] += __popc(msk);
+        }
+    }
     if (bx1 >= 0) {
         atomicMin(&s_bbox[0], bx0); atomicMax(&s_bbox[1], bx1);
         atomicMin(&s_bbox[2], by0); atomicMax(&s_bbox[3], by1);
     }
-    cluster.sync();
-    if (tid == 0 && rank == 0) {
-        int bb[4] = {1 << 30, -1, 1 << 30, -1};
-        uint32_t fl = 0;
-        for (int q = 0; q < RC; ++q) {
-            const int *rb = cluster.map_shared_rank(s_bbox, q);
-            bb[0] = min(bb[0], rb[0]); bb[1] = max(bb[1], rb[1]);
-            bb[2] = min(bb[2], rb[2]); bb[3] = max(bb[3], rb[3]);
-            fl |= *cluster.map_shared_rank(&s_flags, q);
-        }
-        ctl.epoch = epoch;
+    __syncthreads();
+    if (epoch == TAG_MAX) {
+        // tag range used up: the next raster starts from a cleared z-buffer
+        for (int p = tid; p < NPIX; p += RR_THREADS) zb[p] = ~0ull;
+    }
+    if (tid == 0) {
+        const uint32_t fl = s_flags;
+        ctl.epoch = epoch == TAG_MAX ? 0u : epoch;
         ctl.flags |= fl;
         ctl.renders += 1;
-        for (int q = 0; q < 4; ++q) ctl.bbox[q] = bb[q];
-        if (bb[1] >= 0 && (bb[0] < 1 || bb[1] > DIM - 2 || bb[2] < 1 || bb[3] > DIM - 2))
+        for (int q = 0; q < 4; ++q) ctl.bbox[q] = s_bbox[q];
+        if (s_bbox[1] >= 0 && (s_bbox[0] < 1 || s_bbox[1] > DIM - 2 || s_bbox[2] < 1 || s_bbox[3] > DIM - 2))
             ctl.flags |= FLAG_OUT_OF_DOMAIN;
         if (fl & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) ctl.render = 0;
     }
-    cluster.sync();   // keep shared memory alive until rank 0 has read it
 }
 
 // ------------------------------------------------------------------------------------------

@@ -23,6 +23,8 @@
 namespace tdi {
 
 constexpr int NOALLOC_MAX_TRIANGLES = 131072;
+constexpr int NA_RC = 8;          // blocks of the frame's cluster
+constexpr int NA_WARPS = 32;      // warps per block
 
 struct NoAllocScratch {
     unsigned long long zbuf[NPIX];                 // depth keys of the crop (512 KiB)
@@ -31,10 +33,10 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// The raster of k_raster for a single frame: same passes, same slot order, same owner rule,
-// with the scratch above and the caller's output arrays (16-byte records: pixel | owner<<31,
+// The batch raster's algorithm for a single frame, as one cluster: same fragment order, same
+// slot order, same owner rule, with the scratch above and the caller's output arrays (16-byte records: pixel | owner<<31,
 // triangle, float bits of alpha and beta).
-__global__ void __cluster_dims__(RC, 1, 1) __launch_bounds__(1024)
+__global__ void __cluster_dims__(NA_RC, 1, 1) __launch_bounds__(1024)
 k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_t *tl, int T,
                  int x0, int y0, NoAllocScratch *scr, int32_t *frags, int capacity,
                  int32_t *count, uint32_t *flags_out)
@@ -42,8 +44,8 @@ k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
-    __shared__ uint32_t s_cnt[RWARPS][NTMP];
-    __shared__ uint32_t s_off[RWARPS][NTMP];
+    __shared__ uint32_t s_cnt[NA_WARPS][NTMP];
+    __shared__ uint32_t s_off[NA_WARPS][NTMP];
     __shared__ uint32_t s_blk[NTMP];
     __shared__ int s_bbox[4];
     __shared__ uint32_t s_flags;
@@ -59,13 +61,13 @@ k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_
         s_bbox[1] = s_bbox[3] = -1;
     }
     // the array keeps the previous call's keys: reset them (every key below compares smaller)
-    for (int p = rank * 1024 + tid; p < NPIX; p += RC * 1024) zb[p] = ~0ull;
+    for (int p = rank * 1024 + tid; p < NPIX; p += NA_RC * 1024) zb[p] = ~0ull;
     __threadfence();
     cluster.sync();
     const uint32_t tag = 0;
-    const int gwarps = RC * RWARPS;
+    const int gwarps = NA_RC * NA_WARPS;
     const int per_warp = ((T + gwarps * 32 - 1) / (gwarps * 32)) * 32;
-    const int t_begin = (rank * RWARPS + warp) * per_warp;
+    const int t_begin = (rank * NA_WARPS + warp) * per_warp;
     const int t_end = min(T, t_begin + per_warp);
     uint32_t flags = 0;
     int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
@@ -107,14 +109,14 @@ k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_
     __syncthreads();
     if (tid < NTMP) {
         uint32_t tot = 0;
-        for (int w = 0; w < RWARPS; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
+        for (int w = 0; w < NA_WARPS; ++w) { s_off[w][tid] = tot; tot += s_cnt[w][tid]; }
         s_blk[tid] = tot;
     }
     cluster.sync();
     uint32_t rowbase[NTMP], blkoff[NTMP];
     {
         uint32_t tot[NTMP] = {0, 0, 0, 0};
-        for (int q = 0; q < RC; ++q) {
+        for (int q = 0; q < NA_RC; ++q) {
             const uint32_t *rb = cluster.map_shared_rank(s_blk, q);
             for (int r = 0; r < NTMP; ++r) {
                 const uint32_t v = rb[r];
@@ -181,7 +183,7 @@ k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_
     if (tid == 0 && rank == 0) {
         int bb[4] = {1 << 30, -1, 1 << 30, -1};
         uint32_t fl = 0;
-        for (int q = 0; q < RC; ++q) {
+        for (int q = 0; q < NA_RC; ++q) {
             const int *rb = cluster.map_shared_rank(s_bbox, q);
             bb[0] = min(bb[0], rb[0]); bb[1] = max(bb[1], rb[1]);
             bb[2] = min(bb[2], rb[2]); bb[3] = max(bb[3], rb[3]);
@@ -232,7 +234,7 @@ extern "C" tdi_status tdi_raster_noalloc(const float *xp, const float *yp, const
         }
         scr = g_noalloc_ptr[dev];
     }
-    k_raster_noalloc<<<RC, 1024, 0, (cudaStream_t)stream>>>(xp, yp, zc, triangles, n_triangles, x0, y0,
+    k_raster_noalloc<<<NA_RC, 1024, 0, (cudaStream_t)stream>>>(xp, yp, zc, triangles, n_triangles, x0, y0,
                                                             scr, fragments, capacity, count, flags);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(TDI_ERR_CUDA, std::string("tdi_raster_noalloc: launch: ") + cudaGetErrorString(e));

@@ -4,11 +4,14 @@ The BFM'09 files that 3DI fits with are licence-gated and absent, so every input
 is generated from a seed with the shapes and value distributions of the real model:
 
 * geometry: ``V`` vertices on a face-like ellipsoid cap (half-axes a=0.08 m, b=0.10 m,
-  depth c=0.05 m; the cap bulges toward the camera), Delaunay-triangulated and trimmed
-  to ``T`` triangles by dropping the outermost ones;
-* bases: smooth Gaussian random fields (a handful of random cosine modes each), scaled so
-  every component has standard deviation ``0.01 * k**-0.5`` (k = 1-based component index);
-  79 expression components, 199 identity and 199 texture components (albedo mean 0.6);
+  depth c=0.05 m; the cap bulges toward the camera) with a nose, eye sockets and a brow
+  ridge, Delaunay-triangulated and trimmed to ``T`` triangles by dropping the outermost ones;
+* bases: smooth Gaussian random fields (a handful of random cosine modes each, spatial
+  frequency rising slowly with the component index k), scaled so every component has
+  standard deviation ``0.006 / k`` m (k = 1-based); the deformed meshes stay unfolded like
+  a real face mesh (total projected triangle area within ~10% of the covered area);
+  79 expression components and 199 identity components; the albedo is 0.62 plus a
+  mottled random field, darker at the eyes, brows, nostrils and lips;
 * the subject is mean + identity deformation, fixed for the video fit, exactly like the
   ``.shp``/``.tex`` identity files that ``video_from_saved_identity`` loads
   (src/apps/video_from_saved_identity.cu:141-150);
@@ -115,13 +118,28 @@ class Frames:
         return self.xl.shape[0]
 
 
-def _smooth_fields(rng, uv, n_fields, std, n_modes=5):
-    """n_fields smooth random fields over points uv [V,2], each with per-point std ``std[i]``."""
+def _blob(u, v, cu, cv, su, sv):
+    """Gaussian bump of height 1 centred at (cu, cv) with half-widths (su, sv) in (u, v)."""
+    return np.exp(-(((u - cu) / su) ** 2 + ((v - cv) / sv) ** 2))
+
+
+def _face_relief(u, v):
+    """Height of nose ridge and tip, eye sockets and brow ridge toward the camera (metres)."""
+    r = 0.022 * _blob(u, v, 0.0, -0.08, 0.085, 0.24) + 0.006 * _blob(u, v, 0.0, -0.28, 0.12, 0.06)
+    r = r - 0.008 * (_blob(u, v, -0.33, 0.22, 0.12, 0.07) + _blob(u, v, 0.33, 0.22, 0.12, 0.07))
+    r = r + 0.004 * (_blob(u, v, -0.33, 0.40, 0.16, 0.05) + _blob(u, v, 0.33, 0.40, 0.16, 0.05))
+    return r
+
+
+def _smooth_fields(rng, uv, n_fields, std, n_modes=5, s_hi=0.04):
+    """n_fields smooth random fields over points uv [V,2], each with per-point std ``std[i]``;
+    the spatial frequency of field k (1-based) has scale 0.25 + s_hi * sqrt(k) cycles per
+    unit of (u, v)."""
     V = uv.shape[0]
     out = np.empty((n_fields, V), dtype=np.float64)
     for i in range(n_fields):
         k = i + 1
-        s = 0.35 + 0.22 * math.sqrt(k)
+        s = 0.25 + s_hi * math.sqrt(k)
         f = rng.normal(0.0, s, size=(n_modes, 2))
         ph = rng.uniform(0, 2 * math.pi, size=n_modes)
         w = rng.normal(0.0, 1.0, size=n_modes)
@@ -132,14 +150,37 @@ def _smooth_fields(rng, uv, n_fields, std, n_modes=5):
     return out
 
 
-def _basis_std(K):
-    return 0.01 * np.arange(1, K + 1, dtype=np.float64) ** -0.5
+def _face_albedo(rng, uv, u, v, beta, n_tex):
+    """Skin albedo with a mottled random field, darker at the eyes, brows, nostrils and lips."""
+    tex = 0.62 + beta @ _smooth_fields(rng, uv, n_tex, 0.05 / np.sqrt(np.arange(1, n_tex + 1)), s_hi=0.25)
+    tex = tex - 0.40 * (_blob(u, v, -0.33, 0.22, 0.09, 0.04) + _blob(u, v, 0.33, 0.22, 0.09, 0.04))
+    tex = tex - 0.30 * (_blob(u, v, -0.33, 0.40, 0.14, 0.025) + _blob(u, v, 0.33, 0.40, 0.14, 0.025))
+    tex = tex - 0.25 * (_blob(u, v, -0.07, -0.25, 0.03, 0.02) + _blob(u, v, 0.07, -0.25, 0.03, 0.02))
+    tex = tex - 0.30 * _blob(u, v, 0.0, -0.48, 0.20, 0.035)
+    tex = np.clip(tex, 0.05, 1.0)
+    return tex
+
+
+def _basis_std(K, rough=False):
+    k = np.arange(1, K + 1, dtype=np.float64)
+    return 0.01 * k ** -0.5 if rough else 0.006 / k
 
 
 def make_model(n_vertices: int, n_triangles: int, config_id: int = 0, n_expr: int = 79,
                n_id: int = 199, n_tex: int = 199, eps_bound: float = 4.5,
-               finetune_coef: float = 2.75) -> Model:
-    """Seeded face-like model with ``n_vertices`` points and ``n_triangles`` triangles."""
+               finetune_coef: float = 2.75, surface: str = "face") -> Model:
+    """Seeded face-like model with ``n_vertices`` points and ``n_triangles`` triangles.
+
+    ``surface="face"`` (default): smooth bases with std 0.006/k m, a relief (nose, eye
+    sockets, brows) and albedo features; deformed meshes stay unfolded. ``surface="rough"``:
+    bases with std 0.01*k**-0.5 m and faster-rising spatial frequency, plain cap and albedo
+    0.6 plus fields of the same std; its deformed meshes fold over themselves (total
+    projected triangle area several times the covered area, about half the triangles facing
+    away), which gives the raster many more overlapping fragments per pixel.
+    """
+    if surface not in ("face", "rough"):
+        raise ValueError(surface)
+    rough = surface == "rough"
     from scipy.spatial import Delaunay
 
     rng = _rng(config_id, 0)
@@ -156,7 +197,11 @@ def make_model(n_vertices: int, n_triangles: int, config_id: int = 0, n_expr: in
     v = r * np.sin(th)
     x = a * u
     y = b * v
+    # cap bulging toward the camera (-z), with a face's relief: nose ridge and tip, eye
+    # sockets, brow ridge (metres)
     z = -c * np.sqrt(np.maximum(1.0 - u * u - v * v, 0.0))
+    if not rough:
+        z = z - _face_relief(u, v)
 
     tri = Delaunay(np.c_[u, v]).simplices.astype(np.int64)
     if tri.shape[0] < n_triangles:
@@ -174,17 +219,21 @@ def make_model(n_vertices: int, n_triangles: int, config_id: int = 0, n_expr: in
 
     uv = np.c_[u, v]
     E = np.empty((V, 3, n_expr), dtype=np.float64)
-    std_e = _basis_std(n_expr)
+    s_hi = 0.22 if rough else 0.04
+    std_e = _basis_std(n_expr, rough)
     for cidx in range(3):
-        E[:, cidx, :] = _smooth_fields(rng, uv, n_expr, std_e).T
+        E[:, cidx, :] = _smooth_fields(rng, uv, n_expr, std_e, s_hi=s_hi).T
     # Identity: only the subject's deformation is needed (identity is fixed in the fit).
-    std_i = _basis_std(n_id)
+    std_i = _basis_std(n_id, rough)
     alpha = np.clip(rng.normal(size=n_id), -3.5, 3.5)
     ident = np.zeros((3, V))
     for cidx in range(3):
-        ident[cidx] = alpha @ _smooth_fields(rng, uv, n_id, std_i)
+        ident[cidx] = alpha @ _smooth_fields(rng, uv, n_id, std_i, s_hi=s_hi)
     beta = np.clip(rng.normal(size=n_tex), -3.5, 3.5)
-    tex = 0.6 + beta @ _smooth_fields(rng, uv, n_tex, _basis_std(n_tex))
+    if rough:
+        tex = 0.6 + beta @ _smooth_fields(rng, uv, n_tex, _basis_std(n_tex, True), s_hi=s_hi)
+    else:
+        tex = _face_albedo(rng, uv, u, v, beta, n_tex)
 
     mean = np.stack([x, y, z]) + ident
 
@@ -389,10 +438,19 @@ def add_noise(images: np.ndarray, sigma: float, config_id: int = 0) -> np.ndarra
 
 # Workloads named after what they are; sizes follow the reference's fitted model class.
 WORKLOADS = {
-    "cap5k_256": dict(n_vertices=5000, n_triangles=9800, config_id=0,
-                      frames=dict(image_wh=(256, 256), tz=0.6)),
-    "cap53k_1080p": dict(n_vertices=53490, n_triangles=106466, config_id=1,
-                         frames=dict(image_wh=(1920, 1080), box_range=(300, 600))),
-    "cap53k_video": dict(n_vertices=53490, n_triangles=106466, config_id=3,
-                         frames=dict(image_wh=(1920, 1080), box_range=(120, 600), ar1=True)),
+    "cap5k_256": dict(model=dict(n_vertices=5000, n_triangles=9800, config_id=0),
+                      frames=dict(config_id=0, image_wh=(256, 256), tz=0.6)),
+    "cap53k_1080p": dict(model=dict(n_vertices=53490, n_triangles=106466, config_id=1),
+                         frames=dict(config_id=1, image_wh=(1920, 1080), box_range=(300, 600))),
+    "cap53k_video": dict(model=dict(n_vertices=53490, n_triangles=106466, config_id=1),
+                         frames=dict(config_id=3, image_wh=(1920, 1080), box_range=(120, 600), ar1=True)),
 }
+
+
+def make_workload(name: str, n_frames: int, seed_offset: int = 0, surface: str = "face"):
+    """Model and frames of a named workload; ``seed_offset`` shifts the frame seeds."""
+    spec = WORKLOADS[name]
+    m = make_model(**spec["model"], surface=surface)
+    fkw = dict(spec["frames"])
+    cid = fkw.pop("config_id") + seed_offset
+    return m, make_frames(m, n_frames, cid, **fkw)

@@ -60,10 +60,7 @@ def dist_setup(args):
 
 
 def make_workload(synth, n_frames, seed_offset=0):
-    spec = synth.WORKLOADS[WORKLOAD]
-    m = synth.make_model(spec["n_vertices"], spec["n_triangles"], spec["config_id"])
-    fr = synth.make_frames(m, n_frames, spec["config_id"] + seed_offset, **spec["frames"])
-    return m, fr
+    return synth.make_workload(WORKLOAD, n_frames, seed_offset)
 
 
 class ClockSampler:

@@ -162,10 +162,10 @@ tdi_status tdi_batch_launches(tdi_batch *b, int64_t *launches);
 
 /* Live timing of one kernel for roofline reports: while kernel_id != 0, every launch of that
  * kernel is bracketed by CUDA events on its stream and the frames it processed are counted
- * on the device. kernel_id: 1 vertex stage, 2 visibility, 3 render, 4 neighbour maps,
- * 5 Jacobian rows, 6 normal equations, 7 barrier terms, 8 Cholesky. profile_read returns the
- * launches, their summed milliseconds and the frames they processed since profile() was
- * called (synchronises). */
+ * on the device. kernel_id: 1 vertex stage, 2 visibility depth pass, 3 render, 4 neighbour
+ * maps, 5 Jacobian rows, 6 normal equations, 7 barrier terms, 8 Cholesky, 9 visibility
+ * resolve (fragment list). profile_read returns the launches, their summed milliseconds and
+ * the frames they processed since profile() was called (synchronises). */
 tdi_status tdi_batch_profile(tdi_batch *b, int32_t kernel_id);
 tdi_status tdi_batch_profile_read(tdi_batch *b, int64_t *launches, double *total_ms,
                                   int64_t *frames);

@@ -33,9 +33,10 @@ def O():
     return oracle
 
 
-def make_case(synth, O, n_vertices, n_triangles, config_id, n_frames, frames_kw, noise=0.02):
+def make_case(synth, O, n_vertices, n_triangles, config_id, n_frames, frames_kw, noise=0.02,
+              surface="face"):
     """Model, frames with noisy targets rendered by the oracle at the true states."""
-    m = synth.make_model(n_vertices, n_triangles, config_id)
+    m = synth.make_model(n_vertices, n_triangles, config_id, surface=surface)
     fr = synth.make_frames(m, n_frames, config_id, **frames_kw)
     om = O.Model(m)
     cfg = O.config()
@@ -58,3 +59,11 @@ def small_case(synth, O):
 def full_case(synth, O):
     """53,490 vertices / 106,466 triangles, 1080p frames rescaled to the 256x256 crop."""
     return make_case(synth, O, 53490, 106466, 1, 2, dict(image_wh=(1920, 1080), box_range=(300, 600)))
+
+
+@pytest.fixture(scope="session")
+def rough_case(synth, O):
+    """The full-size model with rough bases: the mesh folds over itself, so most pixels are
+    covered by several triangles (depth tests, ties and dropped fragments everywhere)."""
+    return make_case(synth, O, 53490, 106466, 1, 2, dict(image_wh=(1920, 1080), box_range=(300, 600)),
+                     surface="rough")

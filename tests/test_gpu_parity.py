@@ -25,7 +25,7 @@ def _bits(a):
     return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
 
 
-@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+@pytest.mark.parametrize("case_name", ["small_case", "full_case", "rough_case"])
 def test_raster_bit_exact_on_same_projections(request, tdi, synth, O, case_name):
     case = request.getfixturevalue(case_name)
     m, fr, om = case
@@ -46,7 +46,7 @@ def test_raster_bit_exact_on_same_projections(request, tdi, synth, O, case_name)
             assert np.array_equal(got["owner"], ref["owner"])
 
 
-@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+@pytest.mark.parametrize("case_name", ["small_case", "full_case", "rough_case"])
 def test_evaluate_matches_oracle(request, tdi, synth, O, case_name):
     case = request.getfixturevalue(case_name)
     m, fr, om = case
@@ -117,3 +117,27 @@ def test_render_skipped_frame_is_flagged_and_left_unchanged(tdi, synth, O, small
     assert rep[0].flags & tdi.FLAG_FAIL
     assert np.array_equal(xo[0], x[0])
     assert not rep[1].flags & tdi.FLAG_RENDER_SKIPPED
+
+
+def test_raster_stays_exact_across_the_depth_key_epoch_wrap(tdi, synth, O, small_case):
+    """The z-buffer is never cleared between rasters: each raster's keys carry an epoch tag
+    that beats all earlier ones, and the buffer is reset when the 13-bit tag range (8,191
+    rasters) is used up. Rasters alternate between two poses across the reset."""
+    m, fr, om = small_case
+    model, batch, lam, L = _setup(tdi, small_case, synth)
+    tag_max = (1 << 13) - 1
+    cases = []
+    for state in (fr.state_true[0], fr.state_init[0]):
+        geo, ok = O.vertex_stage(om, state, fr.cam[0])
+        xp, yp, Z = geo[6], geo[7], geo[5]
+        x0, y0 = (int(v) for v in fr.x0y0[0])
+        cases.append(((xp, yp, Z, x0, y0), O.raster(om, xp, yp, Z, x0, y0)))
+    for it in range(tag_max + 4):
+        args, ref = cases[it & 1]
+        n, flags = batch.raster(0, *args)
+        if it >= tag_max - 3:
+            got = batch.read(0, tdi.READ_FRAGMENTS)
+            assert n == ref["N"], it
+            assert np.array_equal(got["tri"], ref["tri"]), it
+            assert np.array_equal(got["owner"], ref["owner"]), it
+            assert np.array_equal(got["pix"], ref["pix"]), it
