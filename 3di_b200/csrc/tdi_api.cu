@@ -229,7 +229,7 @@ struct Launch {
     int F;
     size_t smem_vertex() const { return (size_t)(3 * m.KP * 33 + VT_F * m.KP) * sizeof(float); }
     size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
-    size_t smem_ne() const { return (size_t)(2 * NE_CHUNK * m.KTP + 2 * NE_CHUNK) * sizeof(float); }
+    size_t smem_ne() const { return (size_t)(2 * NE_SUB * m.KTP + 2 * NE_SUB) * sizeof(double); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
     size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
     dim3 fblocks() const { return dim3((F + 127) / 128); }
@@ -251,7 +251,7 @@ tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
 
 tdi_status geometry(const Launch &L, const Cfg &c, int stage)
 {
-    dim3 vg((L.m.V + VT_V - 1) / VT_V, (L.A() + VT_F - 1) / VT_F);
+    dim3 vg((L.A() + VT_F - 1) / VT_F, (L.m.V + VT_V - 1) / VT_V);
     TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
                    (size_t)PC_WARPS * (2 * L.m.K + 4 * NL) * sizeof(float), L.s, L.m, L.b, c, stage));
@@ -270,7 +270,7 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
 {
     TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
     TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.A()), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_SPLIT, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_BPF, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
@@ -475,7 +475,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
     A(d.ctl, F); A(d.act, F); A(d.geo, F * 6 * md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
-    A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_SPLIT * (size_t)ne_part_stride((int)KTP)); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
+    A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_MAXCH * (size_t)ne_part_stride((int)KTP)); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
     A(d.prof_frames, 1);
 #undef A
     if (st != TDI_OK) return cleanup(st);
@@ -761,7 +761,7 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     TDI_TRY(compact_active(b, s, &n));
     if (n > 0) {
         TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
-        dim3 vg((m.V + VT_V - 1) / VT_V, (n + VT_F - 1) / VT_F);
+        dim3 vg((n + VT_F - 1) / VT_F, (m.V + VT_V - 1) / VT_V);
         TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
         TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, n), dim3(RD_THREADS), 0, s, m, d));
         TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));

@@ -123,7 +123,7 @@ struct DBatch {
     int32_t *nb;             // [F][4][NMAX]: kl, kr, ka, kb
     int32_t *perm;           // [F][NMAX]: sorted position -> fragment
     float *J;                // [F][NMAX][KTP]
-    double *ne_part;         // [F][NE_SPLIT][part stride] partial normal equations
+    double *ne_part;         // [F][NMAX/256][part stride] chunk partials of the normal equations
     float *img;              // [F][2][NPIX] blur scratch for frames too large for shared memory
     // live profiling: frames processed by the kernel being timed (kernel ids as in tdi.h)
     unsigned long long *prof_frames;

@@ -178,25 +178,27 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
     float *Es = vsm;                           // [3*KP][33]: basis rows, vertex-minor
     float *Xs = vsm + 3 * KP * 33;             // [VT_F][KP]: coefficients per frame
     __shared__ int s_any;
-    const int v0 = blockIdx.x * VT_V, f0 = blockIdx.y * VT_F;
+    // frame tiles vary fastest, so the blocks that share a basis tile run together and read
+    // it from L2
+    const int v0 = blockIdx.y * VT_V, f0 = blockIdx.x * VT_F;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     if (tid == 0) s_any = 0;
     __syncthreads();
     if (tid < VT_F && f0 + tid < b.nact && b.ctl[b.act[f0 + tid]].render) {
         s_any = 1;
-        if (blockIdx.x == 0) prof_count(b, KID_VERTEX);
+        if (blockIdx.y == 0) prof_count(b, KID_VERTEX);
     }
     __syncthreads();
     if (!s_any) return;
     const int nv = min(VT_V, m.V - v0);
-    for (int i = tid; i < VT_V * 3 * KP; i += 256) {
-        int vl = i / (3 * KP), rem = i - vl * 3 * KP;
-        Es[rem * 33 + vl] = vl < nv ? m.E[(size_t)(v0 + vl) * 3 * KP + rem] : 0.0f;
+    for (int vl = threadIdx.y; vl < VT_V; vl += 8) {
+        const float *er = m.E + (size_t)(v0 + vl) * 3 * KP;
+        for (int rem = threadIdx.x; rem < 3 * KP; rem += 32) Es[rem * 33 + vl] = vl < nv ? er[rem] : 0.0f;
     }
-    for (int i = tid; i < VT_F * KP; i += 256) {
-        int fl = i / KP, k = i - fl * KP;
+    for (int fl = threadIdx.y; fl < VT_F; fl += 8) {
         const int ai = f0 + fl;
-        Xs[i] = (ai < b.nact && k < K) ? b.xe[(size_t)b.act[ai] * m.KTP + k] : 0.0f;
+        const float *xr = ai < b.nact ? b.xe + (size_t)b.act[ai] * m.KTP : nullptr;
+        for (int k = threadIdx.x; k < KP; k += 32) Xs[fl * KP + k] = (xr && k < K) ? xr[k] : 0.0f;
     }
     __syncthreads();
     const int vl = threadIdx.x;
@@ -1179,13 +1181,21 @@ __device__ __forceinline__ void chain(const float *Jf, int ld, const int32_t *nb
 }
 
 // ------------------------------------------------------------------------------------------
-// Normal equations of the image term (derivative_computer.cu:135-164), one block per frame:
-// rows of d(gx/|g|)/dtheta and d(gy/|g|)/dtheta are formed 32 fragments at a time in shared
-// memory and folded into H = tau * sum(row row^T) and g = -tau * sum(w row) with FP64
-// accumulation (4x4 register blocks of the upper triangle per thread).
+// Normal equations of the image term (derivative_computer.cu:135-164): rows of
+// d(gx/|g|)/dtheta and d(gy/|g|)/dtheta, H = tau * sum(row row^T), g = -tau * sum(w row).
+// The reference sums with cublasSgemm in the library's order; the order here is fixed and
+// shared with the oracle: fragments in chunks of NE_CH, each chunk summed from zero with one
+// FP64 fused multiply-add per row and entry in fragment order (x row, then y row), the chunk
+// sums then added in chunk order. The rows are floats, so every product is exact in FP64.
+// k_normal_eq writes one partial per chunk (NE_BPF blocks per frame, each looping over
+// chunks); rows are staged 32 fragments at a time in shared memory as doubles and every
+// thread owns a 4x4 block of the upper triangle. k_normal_eq_reduce adds the chunk partials.
 
-constexpr int NE_THREADS = 256, NE_CHUNK = 32;
-constexpr int NE_SPLIT = 16;                 // blocks per frame, each over a range of fragments
+constexpr int NE_THREADS = 256;
+constexpr int NE_CH = 256;                   // fragments per chunk (the unit of the sum order)
+constexpr int NE_SUB = 32;                   // fragments staged in shared memory at a time
+constexpr int NE_BPF = 16;                   // blocks per frame
+constexpr int NE_MAXCH = NMAX / NE_CH;       // chunk partials per frame at most
 
 // Upper-triangle 4x4 block (bi <= bj) owned by thread t, or -1.
 __device__ __forceinline__ void ne_block(int t, int nb4, int &bi, int &bj)
@@ -1203,83 +1213,136 @@ __host__ __device__ __forceinline__ int ne_part_stride(int KTP)
     return nb4 * (nb4 + 1) / 2 * 16 + KTP;
 }
 
-// Partial sums of one fragment range: sum(row row^T) for the upper 4x4 blocks and
-// sum(w row), FP64, written to b.ne_part[f][split].
-__global__ void __launch_bounds__(NE_THREADS) k_normal_eq(DModel m, DBatch b)
+__global__ void __launch_bounds__(NE_THREADS, 3) k_normal_eq(DModel m, DBatch b)
 {
-    const int f = b.act[blockIdx.y], split = blockIdx.x;
+    const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
-    if (split == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
-    extern __shared__ float nesm[];
+    if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
+    extern __shared__ __align__(16) double nesm[];
     const int KTP = m.KTP, KT = m.KT;
-    float *rows = nesm;                          // [2*NE_CHUNK][KTP]
-    float *wts = rows + 2 * NE_CHUNK * KTP;      // [2*NE_CHUNK]
-    const int tid = threadIdx.x;
+    double *rows = nesm;                         // [2*NE_SUB][KTP]
+    double *wts = rows + 2 * NE_SUB * KTP;       // [2*NE_SUB]
+    __shared__ int s_nb[4][NE_SUB];              // kl, kr, ka, kb
+    __shared__ float s_pre[NE_SUB], s_dx[NE_SUB], s_dy[NE_SUB];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb4 = KTP / 4;
     int bi, bj;
     ne_block(tid, nb4, bi, bj);
-    double acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    double gacc = 0.0;
     const int N = ctl.N;
-    const int per = ((N + NE_SPLIT * NE_CHUNK - 1) / (NE_SPLIT * NE_CHUNK)) * NE_CHUNK;
-    const int nbeg = split * per, nend = min(N, nbeg + per);
+    const int nch = (N + NE_CH - 1) / NE_CH;
     const float *Jf = b.J + (size_t)f * NMAX * KTP;
     const int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
     const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
-    for (int n0 = nbeg; n0 < nend; n0 += NE_CHUNK) {
-        const int cn = min(NE_CHUNK, nend - n0);
-        for (int i = tid; i < NE_CHUNK * KTP; i += NE_THREADS) {
-            const int q = i / KTP, j = i - q * KTP;
-            float ox = 0.0f, oy = 0.0f;
-            if (q < cn && j < KT) {
-                const int n = n0 + q;
-                const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
-                const float pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
-                chain(Jf, KTP, nb, n, j, gx, gy, pre, ox, oy);
-            }
-            rows[(2 * q) * KTP + j] = ox;
-            rows[(2 * q + 1) * KTP + j] = oy;
-        }
-        for (int q = tid; q < NE_CHUNK; q += NE_THREADS) {
-            wts[2 * q] = q < cn ? fg[3 * NMAX + n0 + q] : 0.0f;
-            wts[2 * q + 1] = q < cn ? fg[4 * NMAX + n0 + q] : 0.0f;
-        }
-        __syncthreads();
-        if (bi >= 0) {
-            for (int q = 0; q < cn; ++q) {
-                const float4 ax = *reinterpret_cast<const float4 *>(rows + (2 * q) * KTP + 4 * bi);
-                const float4 cx = *reinterpret_cast<const float4 *>(rows + (2 * q) * KTP + 4 * bj);
-                const float4 ay = *reinterpret_cast<const float4 *>(rows + (2 * q + 1) * KTP + 4 * bi);
-                const float4 cy = *reinterpret_cast<const float4 *>(rows + (2 * q + 1) * KTP + 4 * bj);
-                const double axv[4] = {ax.x, ax.y, ax.z, ax.w}, cxv[4] = {cx.x, cx.y, cx.z, cx.w};
-                const double ayv[4] = {ay.x, ay.y, ay.z, ay.w}, cyv[4] = {cy.x, cy.y, cy.z, cy.w};
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] += axv[i] * cxv[j] + ayv[i] * cyv[j];
-            }
-        }
-        if (tid < KTP) {
-            for (int q = 0; q < cn; ++q)
-                gacc += (double)wts[2 * q] * (double)rows[(2 * q) * KTP + tid] +
-                        (double)wts[2 * q + 1] * (double)rows[(2 * q + 1) * KTP + tid];
-        }
-        __syncthreads();
-    }
     const int stride = ne_part_stride(KTP);
-    double *part = b.ne_part + ((size_t)f * NE_SPLIT + split) * stride;
-    if (bi >= 0)
+    for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+        double acc[4][4];
+#pragma unroll
         for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) part[tid * 16 + i * 4 + j] = acc[i][j];
-    if (tid < KTP) part[nb4 * (nb4 + 1) / 2 * 16 + tid] = gacc;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        double gacc = 0.0;
+        const int c0 = ch * NE_CH, c1 = min(N, c0 + NE_CH);
+        for (int n0 = c0; n0 < c1; n0 += NE_SUB) {
+            const int cn = min(NE_SUB, c1 - n0);
+            // per-fragment scalars and neighbour indices
+            if (tid < NE_SUB) {
+                const int q = tid, n = n0 + q;
+                float pre = 0.0f, dx = 0.0f, dy = 0.0f, wx = 0.0f, wy = 0.0f;
+                int k0 = 0, k1 = 0, k2 = 0, k3 = 0;
+                if (q < cn) {
+                    const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
+                    pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
+                    dx = 2 * gx;
+                    dy = 2 * gy;
+                    wx = fg[3 * NMAX + n];
+                    wy = fg[4 * NMAX + n];
+                    k0 = nb[n]; k1 = nb[NMAX + n]; k2 = nb[2 * NMAX + n]; k3 = nb[3 * NMAX + n];
+                }
+                s_pre[q] = pre; s_dx[q] = dx; s_dy[q] = dy;
+                s_nb[0][q] = k0; s_nb[1][q] = k1; s_nb[2][q] = k2; s_nb[3][q] = k3;
+                wts[2 * q] = (double)wx;
+                wts[2 * q + 1] = (double)wy;
+            }
+            __syncthreads();
+            // rows: warp w builds fragments w, w+8, w+16, w+24, lanes take columns; the four
+            // neighbour rows of two fragments are loaded before any is used
+            for (int cb = 0; cb < KTP; cb += 96)
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                float v[2][3][4];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int q = warp + 8 * (2 * half + i);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int j = cb + lane + 32 * c;
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            v[i][c][r] = (q < cn && j < KT) ? Jf[(size_t)s_nb[r][q] * KTP + j] : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int q = warp + 8 * (2 * half + i);
+                    const float pre = s_pre[q], diffx = s_dx[q], diffy = s_dy[q];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int j = cb + lane + 32 * c;
+                        if (j >= KTP) continue;
+                        float ox = 0.0f, oy = 0.0f;
+                        if (q < cn && j < KT) {
+                            const float dh = v[i][c][1] - v[i][c][0];
+                            const float dv = v[i][c][3] - v[i][c][2];
+                            const float X = (-diffy) * (-dh) - (-diffx) * (-dv);
+                            ox = ((-pre) * (-diffy)) * X;
+                            oy = (pre * (-diffx)) * X;
+                        }
+                        rows[(2 * q) * KTP + j] = (double)ox;
+                        rows[(2 * q + 1) * KTP + j] = (double)oy;
+                    }
+                }
+            }
+            __syncthreads();
+            if (bi >= 0) {
+                for (int q = 0; q < cn; ++q) {
+                    const double *rx = rows + (2 * q) * KTP, *ry = rx + KTP;
+                    const double2 ax0 = *reinterpret_cast<const double2 *>(rx + 4 * bi);
+                    const double2 ax1 = *reinterpret_cast<const double2 *>(rx + 4 * bi + 2);
+                    const double2 cx0 = *reinterpret_cast<const double2 *>(rx + 4 * bj);
+                    const double2 cx1 = *reinterpret_cast<const double2 *>(rx + 4 * bj + 2);
+                    const double2 ay0 = *reinterpret_cast<const double2 *>(ry + 4 * bi);
+                    const double2 ay1 = *reinterpret_cast<const double2 *>(ry + 4 * bi + 2);
+                    const double2 cy0 = *reinterpret_cast<const double2 *>(ry + 4 * bj);
+                    const double2 cy1 = *reinterpret_cast<const double2 *>(ry + 4 * bj + 2);
+                    const double axv[4] = {ax0.x, ax0.y, ax1.x, ax1.y}, cxv[4] = {cx0.x, cx0.y, cx1.x, cx1.y};
+                    const double ayv[4] = {ay0.x, ay0.y, ay1.x, ay1.y}, cyv[4] = {cy0.x, cy0.y, cy1.x, cy1.y};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(ayv[i], cyv[j], fma(axv[i], cxv[j], acc[i][j]));
+                }
+            }
+            if (tid < KTP) {
+                for (int q = 0; q < cn; ++q)
+                    gacc = fma(wts[2 * q + 1], rows[(2 * q + 1) * KTP + tid], fma(wts[2 * q], rows[(2 * q) * KTP + tid], gacc));
+            }
+            __syncthreads();
+        }
+        double *part = b.ne_part + ((size_t)f * NE_MAXCH + ch) * stride;
+        if (bi >= 0) {
+            double2 *o = reinterpret_cast<double2 *>(part + tid * 16);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                o[2 * i] = make_double2(acc[i][0], acc[i][1]);
+                o[2 * i + 1] = make_double2(acc[i][2], acc[i][3]);
+            }
+        }
+        if (tid < KTP) part[nb4 * (nb4 + 1) / 2 * 16 + tid] = gacc;
+    }
 }
 
-// Sum of the partial normal equations in split order: H = tau*S, g = -tau*w.
+// Sum of the chunk partials in chunk order: H = tau*S, g = -tau*w.
 __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatch b)
 {
     const int f = b.act[blockIdx.x];
@@ -1288,26 +1351,37 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatc
     const int KTP = m.KTP, KT = m.KT, tid = threadIdx.x;
     const int nb4 = KTP / 4;
     const int stride = ne_part_stride(KTP);
-    const double *part = b.ne_part + (size_t)f * NE_SPLIT * stride;
+    const int nch = (ctl.N + NE_CH - 1) / NE_CH;
+    const double *part = b.ne_part + (size_t)f * NE_MAXCH * stride;
     const double tau = 25.0;
     float *H = b.H + (size_t)f * KTP * KTP;
     int bi, bj;
     ne_block(tid, nb4, bi, bj);
     if (bi >= 0) {
+        double s[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) s[e] = 0.0;
+        for (int q = 0; q < nch; ++q) {
+            const double2 *p = reinterpret_cast<const double2 *>(part + (size_t)q * stride + tid * 16);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const double2 v = p[e];
+                s[2 * e] += v.x;
+                s[2 * e + 1] += v.y;
+            }
+        }
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 4; ++j) {
-                double s = 0.0;
-                for (int q = 0; q < NE_SPLIT; ++q) s += part[(size_t)q * stride + tid * 16 + i * 4 + j];
                 const int a = 4 * bi + i, c = 4 * bj + j;
                 if (a >= KT || c >= KT) continue;
-                const float v = (float)(tau * s);
+                const float v = (float)(tau * s[i * 4 + j]);
                 H[(size_t)a * KTP + c] = v;
                 H[(size_t)c * KTP + a] = v;
             }
     }
     if (tid < KT) {
         double s = 0.0;
-        for (int q = 0; q < NE_SPLIT; ++q) s += part[(size_t)q * stride + nb4 * (nb4 + 1) / 2 * 16 + tid];
+        for (int q = 0; q < nch; ++q) s += part[(size_t)q * stride + nb4 * (nb4 + 1) / 2 * 16 + tid];
         b.g[(size_t)f * KTP + tid] = (float)(-tau * s);
     }
 }

@@ -336,46 +336,48 @@ def main():
                 "failed": int(sum(1 for r in rep if r.flags & tdi.FLAG_FAIL))},
     }
     if rank == 0 and world == 1:
-        # plain form: the same frames fitted one at a time (a batch of one per fit)
         nplain = min(args.plain_frames, F)
-        one = tdi.Batch(model, 1)
-        plain_ms = 0.0
-        for i in range(nplain):
-            one.set_frames(fr, i, i + 1)
-            one.set_state(fr.state_init[i:i + 1], lam0[i:i + 1], L[i:i + 1])
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            one.fit(cfg)
-            e1.record()
-            torch.cuda.synchronize()
-            plain_ms += e0.elapsed_time(e1)
-        one.close()
-        line["plain"] = {"value": nplain / (plain_ms / 1000.0), "unit": "frames/s",
-                         "frames": nplain, "note": "unbatched: one frame per fit, same kernels"}
-        line["batched_over_plain"] = value / line["plain"]["value"]
+        if nplain > 0:
+            # plain form: the same frames fitted one at a time (a batch of one per fit)
+            one = tdi.Batch(model, 1)
+            plain_ms = 0.0
+            for i in range(nplain):
+                one.set_frames(fr, i, i + 1)
+                one.set_state(fr.state_init[i:i + 1], lam0[i:i + 1], L[i:i + 1])
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                one.fit(cfg)
+                e1.record()
+                torch.cuda.synchronize()
+                plain_ms += e0.elapsed_time(e1)
+            one.close()
+            line["plain"] = {"value": nplain / (plain_ms / 1000.0), "unit": "frames/s",
+                             "frames": nplain, "note": "unbatched: one frame per fit, same kernels"}
+            line["batched_over_plain"] = value / line["plain"]["value"]
 
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        O.build()
-        n = min(args.cpu_frames, F)
-        threads = O.max_threads()
-        rate = cpu_fit_rate(O, synth, m, fr, n, threads)
-        line["cpu_baseline"] = {"value": rate, "unit": "frames/s", "cores": threads, "kind": "port",
-                                "sample": f"first {n} frames of the same batch, FP32 CPU restatement"}
-        # parameter error of the GPU fit against the FP32 and FP64 oracles on those frames
-        om = O.Model(m)
-        fs = O.FrameSet(fr, 0, n)
-        ocfg = O.config(max_iters_rigid=MAX_ITERS)
-        errs = {}
-        for kind in ("f32", "f64"):
-            ox, ol, orep = O.fit_frames(om, fs, ocfg, fr.state_init[:n], lam0[:n], L[:n], kind=kind)
-            rel = np.abs(x[:n] - ox) / np.maximum(np.abs(ox), 1e-2)
-            errs[kind] = {"max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
-                          "frames_within_1e-5": int(np.sum(rel.max(axis=1) <= 1e-5))}
-        line["param_err"] = {"frames": n, "vs_fp32_oracle": errs["f32"], "vs_fp64_oracle": errs["f64"],
-                             "definition": "|x_gpu - x_oracle| / max(|x_oracle|, 1e-2) over pose and expressions"}
+        if args.cpu_frames > 0:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            O.build()
+            n = min(args.cpu_frames, F)
+            threads = O.max_threads()
+            rate = cpu_fit_rate(O, synth, m, fr, n, threads)
+            line["cpu_baseline"] = {"value": rate, "unit": "frames/s", "cores": threads, "kind": "port",
+                                    "sample": f"first {n} frames of the same batch, FP32 CPU restatement"}
+            # parameter error of the GPU fit against the FP32 and FP64 oracles on those frames
+            om = O.Model(m)
+            fs = O.FrameSet(fr, 0, n)
+            ocfg = O.config(max_iters_rigid=MAX_ITERS)
+            errs = {}
+            for kind in ("f32", "f64"):
+                ox, ol, orep = O.fit_frames(om, fs, ocfg, fr.state_init[:n], lam0[:n], L[:n], kind=kind)
+                rel = np.abs(x[:n] - ox) / np.maximum(np.abs(ox), 1e-2)
+                errs[kind] = {"max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+                              "frames_within_1e-5": int(np.sum(rel.max(axis=1) <= 1e-5))}
+            line["param_err"] = {"frames": n, "vs_fp32_oracle": errs["f32"], "vs_fp64_oracle": errs["f64"],
+                                 "definition": "|x_gpu - x_oracle| / max(|x_oracle|, 1e-2) over pose and expressions"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     batch.close()

@@ -803,18 +803,38 @@ static void image_normal_equations(ctx_t *c, real tau, real *H, real *gvec)
     o_neighbours(c->fr.pix, N, c->nb, &fl);
     c->rep->flags |= fl;
     jacobian_rows(m, &c->fr, c->sh, c->g, c->R, c->dR, cam, c->J);
+    /* The reference forms H and g with cublasSgemm (derivative_computer.cu:157-163), whose
+     * summation order is the library's. The order here is fixed: fragments in chunks of
+     * NE_CHUNK; within a chunk, from zero, one fused multiply-add per row and entry in fragment
+     * order (x row, then y row); the chunk sums are then added in chunk order. In the FP32
+     * build the rows are floats, so every product is exact in double and only the additions
+     * round. */
+    enum { NE_CHUNK = 256 };
     double *Hs = (double *)calloc((size_t)KT * KT, sizeof(double));
     double *gs = (double *)calloc(KT, sizeof(double));
+    double *Hc = (double *)malloc(sizeof(double) * (size_t)KT * KT);
+    double *gc = (double *)malloc(sizeof(double) * KT);
     real *gxr = (real *)malloc(sizeof(real) * KT), *gyr = (real *)malloc(sizeof(real) * KT);
-    for (int n = 0; n < N; ++n) {
-        chain_rows(c->J, KT, KT, c->nb, N, n, c->g, gxr, gyr);
-        const double sx = c->g[G_GXSN * N + n], sy = c->g[G_GYSN * N + n];
+    for (int c0 = 0; c0 < N; c0 += NE_CHUNK) {
+        const int c1 = c0 + NE_CHUNK < N ? c0 + NE_CHUNK : N;
+        memset(Hc, 0, sizeof(double) * (size_t)KT * KT);
+        memset(gc, 0, sizeof(double) * KT);
+        for (int n = c0; n < c1; ++n) {
+            chain_rows(c->J, KT, KT, c->nb, N, n, c->g, gxr, gyr);
+            const double sx = c->g[G_GXSN * N + n], sy = c->g[G_GYSN * N + n];
+            for (int a = 0; a < KT; ++a) {
+                const double xa = gxr[a], ya = gyr[a];
+                gc[a] = fma(sy, ya, fma(sx, xa, gc[a]));
+                double *hr = Hc + (size_t)a * KT;
+                for (int b = 0; b <= a; ++b) hr[b] = fma(ya, (double)gyr[b], fma(xa, (double)gxr[b], hr[b]));
+            }
+        }
         for (int a = 0; a < KT; ++a) {
-            const double xa = gxr[a], ya = gyr[a];
-            gs[a] += sx * xa + sy * ya;
-            for (int b = 0; b <= a; ++b) Hs[(size_t)a * KT + b] += xa * gxr[b] + ya * gyr[b];
+            gs[a] += gc[a];
+            for (int b = 0; b <= a; ++b) Hs[(size_t)a * KT + b] += Hc[(size_t)a * KT + b];
         }
     }
+    free(Hc); free(gc);
     for (int a = 0; a < KT; ++a) {
         gvec[a] = (real)(-(double)tau * gs[a]);
         for (int b = 0; b <= a; ++b) {
