@@ -7,6 +7,7 @@
 // accepted gets its normal equations in the same round: the accepted trial's render is the
 // render the next outer iteration of the reference would redo at the same point.
 #include "tdi_kernels.cu"
+#include "tdi_normal_tc.cu"
 
 #include "../../include/tdi.h"
 
@@ -94,6 +95,17 @@ __global__ void k_scalars(DBatch b, double *out)   // [F][4]
     out[f * 4 + 3] = (double)c.face_ok;
 }
 
+// Configuration values the library cannot run with.
+tdi_status check_cfg(const tdi_fit_config &c, const DModel &m)
+{
+    if (c.normal_eq != 0 && c.normal_eq != 1) return fail(TDI_ERR_INVALID, "normal_eq must be 0 or 1");
+    if (c.normal_eq == 1 && m.KT + 1 > TC_MAXN)
+        return fail(TDI_ERR_INVALID, "tensor-core normal equations take at most 121 expression components");
+    if (c.normal_eq == 0 && m.KTP > 8 * NE_GRP)
+        return fail(TDI_ERR_INVALID, "exact normal equations take at most 82 expression components");
+    return TDI_OK;
+}
+
 Cfg to_cfg(const tdi_fit_config &c)
 {
     Cfg r;
@@ -105,6 +117,7 @@ Cfg to_cfg(const tdi_fit_config &c)
     r.max_iters_lambda = c.max_iters_lambda;
     r.ref_face_size = c.ref_face_size;
     for (int i = 0; i < NTAPS; ++i) r.taps[i] = c.taps[i];
+    r.normal_eq = c.normal_eq;
     return r;
 }
 
@@ -217,6 +230,8 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_precheck, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<NE_GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<TC_MAXN / 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     done = true;
     return TDI_OK;
 }
@@ -229,7 +244,7 @@ struct Launch {
     int F;
     size_t smem_vertex() const { return (size_t)(3 * m.KP * 33 + VT_F * m.KP) * sizeof(float); }
     size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
-    size_t smem_ne() const { return (size_t)(2 * NE_SUB * m.KTP + 2 * NE_SUB) * sizeof(double); }
+    size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * m.KTP * sizeof(double); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
     size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
     dim3 fblocks() const { return dim3((F + 127) / 128); }
@@ -242,8 +257,9 @@ struct Launch {
 tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
 {
     TDI_TRY(launch(bt, 0, k_compact_active, dim3(1), dim3(1024), 0, s, (const DBatch)bt->d, bt->d_count));
-    TDI_CUDA(cudaMemcpyAsync(bt->h_count, bt->d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaMemcpyAsync(bt->h_count, bt->d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     TDI_CUDA(cudaStreamSynchronize(s));
+    if (bt->h_count[1]) return fail(TDI_ERR_CUDA, "a tensor-core wait in the normal equations gave up");
     *n = *bt->h_count;
     bt->d.nact = *n;
     return TDI_OK;
@@ -270,8 +286,20 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
 {
     TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
     TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.A()), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_BPF, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));
+    if (c.normal_eq == 1) {
+        // column groups of 8 per thread: 11 cover the reference's 79 expressions and the
+        // weight column
+        if (L.m.KT + 1 <= 8 * NE_GRP)
+            TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq_tc<NE_GRP>, dim3(TC_BPF, L.A()), dim3(TC_THREADS),
+                           (size_t)TC_SMEM, L.s, L.m, L.b));
+        else
+            TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq_tc<TC_MAXN / 8>, dim3(TC_BPF, L.A()), dim3(TC_THREADS),
+                           (size_t)TC_SMEM, L.s, L.m, L.b));
+        TDI_TRY(launch(L.bt, 0, k_normal_eq_tc_reduce, dim3(L.A()), dim3(256), 0, L.s, L.m, L.b));
+    } else {
+        TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_BPF, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
+        TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));
+    }
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
     TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(128), L.smem_solve(), L.s, L.m, L.b, c, stage));
@@ -475,13 +503,14 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
     A(d.ctl, F); A(d.act, F); A(d.geo, F * 6 * md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
-    A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_MAXCH * (size_t)ne_part_stride((int)KTP)); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 1);
+    A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8)); A(d.err, 1); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 2);
     A(d.prof_frames, 1);
 #undef A
     if (st != TDI_OK) return cleanup(st);
-    if (cudaMallocHost(&b->h_count, sizeof(int)) != cudaSuccess) return cleanup(fail(TDI_ERR_NOMEM, "pinned alloc"));
+    if (cudaMallocHost(&b->h_count, 2 * sizeof(int)) != cudaSuccess) return cleanup(fail(TDI_ERR_NOMEM, "pinned alloc"));
     if (cudaMemset(d.zbuf, 0xFF, F * NPIX * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemset(d.ctl, 0, F * sizeof(FrameCtl)) != cudaSuccess ||
+        cudaMemset(d.err, 0, sizeof(int32_t)) != cudaSuccess ||
         cudaMemset(d.tri_mask, 0, F * mask_words(md.T) * sizeof(uint32_t)) != cudaSuccess ||
         cudaMemset(d.x, 0, F * KTP * sizeof(float)) != cudaSuccess ||
         cudaMemset(d.x_ls, 0, F * KTP * sizeof(float)) != cudaSuccess ||
@@ -567,6 +596,7 @@ tdi_status tdi_batch_set_state(tdi_batch *b, const float *x, const float *lam, c
 tdi_status tdi_batch_fit(tdi_batch *b, const tdi_fit_config *cfg, void *stream)
 {
     if (!b || !cfg) return fail(TDI_ERR_INVALID, "null argument");
+    TDI_TRY(check_cfg(*cfg, b->m->d));
     cudaStream_t s = (cudaStream_t)stream;
     const Cfg c = to_cfg(*cfg);
     const dim3 fb((b->d.F + 127) / 128);
@@ -625,6 +655,7 @@ tdi_status tdi_fit_frames(tdi_batch *b, const tdi_frames *frames, const tdi_fit_
 tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t finetune_bounds, void *stream)
 {
     if (!b || !cfg) return fail(TDI_ERR_INVALID, "null argument");
+    TDI_TRY(check_cfg(*cfg, b->m->d));
     cudaStream_t s = (cudaStream_t)stream;
     const Cfg c = to_cfg(*cfg);
     const DModel &m = b->m->d;

@@ -74,6 +74,7 @@ struct Cfg {
         max_iters_lambda;
     float ref_face_size;
     float taps[NTAPS];
+    int32_t normal_eq;       // 0: FP64 in the oracle's order; 1: split-BF16 tensor cores
 };
 
 // Device view of the model.
@@ -128,6 +129,7 @@ struct DBatch {
     // live profiling: frames processed by the kernel being timed (kernel ids as in tdi.h)
     unsigned long long *prof_frames;
     int32_t prof_id;
+    int32_t *err;            // [1] nonzero after a device-side wait gave up
 };
 
 }  // namespace tdi

@@ -4,6 +4,7 @@
 #include "tdi_internal.cuh"
 
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 #include <cfloat>
 #include <cmath>
 
@@ -1194,8 +1195,9 @@ __device__ __forceinline__ void chain(const float *Jf, int ld, const int32_t *nb
 constexpr int NE_THREADS = 256;
 constexpr int NE_CH = 256;                   // fragments per chunk (the unit of the sum order)
 constexpr int NE_SUB = 32;                   // fragments staged in shared memory at a time
-constexpr int NE_BPF = 16;                   // blocks per frame
+constexpr int NE_BPF = 32;                   // blocks per frame
 constexpr int NE_MAXCH = NMAX / NE_CH;       // chunk partials per frame at most
+static_assert(NE_THREADS == NE_CH && NE_SUB == 32 && NE_THREADS == 8 * 32, "thread mapping of the row build");
 
 // Upper-triangle 4x4 block (bi <= bj) owned by thread t, or -1.
 __device__ __forceinline__ void ne_block(int t, int nb4, int &bi, int &bj)
@@ -1213,7 +1215,67 @@ __host__ __device__ __forceinline__ int ne_part_stride(int KTP)
     return nb4 * (nb4 + 1) / 2 * 16 + KTP;
 }
 
-__global__ void __launch_bounds__(NE_THREADS, 3) k_normal_eq(DModel m, DBatch b)
+// Rows of one chunk of NE_CH fragments: per-fragment scalars and neighbour indices are
+// staged once per chunk (one thread per fragment); a thread then builds fragment
+// 4*warp + lane/8 of each 32-fragment stage at columns 8*g + lane%8, its four neighbour
+// rows of J loaded one stage ahead.
+constexpr int NE_GRP = 11;                   // column groups of 8: KTP <= 88 (K <= 82)
+
+struct ChunkHead {
+    int nb[4][NE_CH];
+    float pre[NE_CH], dx[NE_CH], dy[NE_CH];
+    double w[2 * NE_CH];
+};
+
+__device__ __forceinline__ void chunk_head(ChunkHead &hd, const float *fg, const int32_t *nb, int c0, int cnt)
+{
+    const int q = threadIdx.x, n = c0 + q;
+    float pre = 0.0f, dx = 0.0f, dy = 0.0f, wx = 0.0f, wy = 0.0f;
+    int k0 = 0, k1 = 0, k2 = 0, k3 = 0;
+    if (q < cnt) {
+        const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
+        pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
+        dx = 2 * gx;
+        dy = 2 * gy;
+        wx = fg[3 * NMAX + n];
+        wy = fg[4 * NMAX + n];
+        k0 = nb[n]; k1 = nb[NMAX + n]; k2 = nb[2 * NMAX + n]; k3 = nb[3 * NMAX + n];
+    }
+    hd.pre[q] = pre; hd.dx[q] = dx; hd.dy[q] = dy;
+    hd.nb[0][q] = k0; hd.nb[1][q] = k1; hd.nb[2][q] = k2; hd.nb[3][q] = k3;
+    hd.w[2 * q] = (double)wx;
+    hd.w[2 * q + 1] = (double)wy;
+}
+
+template <int GRP>
+__device__ __forceinline__ void chunk_prefetch(float (&v)[GRP][4], const ChunkHead &hd, const float *Jf,
+                                               int KT, int KTP, int q, int cnt, int a_low)
+{
+    const bool live = q < cnt;
+    const int r0 = hd.nb[0][q], r1 = hd.nb[1][q], r2 = hd.nb[2][q], r3 = hd.nb[3][q];
+#pragma unroll
+    for (int g = 0; g < GRP; ++g) {
+        const int a = 8 * g + a_low;
+        const bool use = live && a < KT;
+        v[g][0] = use ? Jf[(size_t)r0 * KTP + a] : 0.0f;
+        v[g][1] = use ? Jf[(size_t)r1 * KTP + a] : 0.0f;
+        v[g][2] = use ? Jf[(size_t)r2 * KTP + a] : 0.0f;
+        v[g][3] = use ? Jf[(size_t)r3 * KTP + a] : 0.0f;
+    }
+}
+
+// Chain rule through the normalised gradient (newfuncs.cu:417-463) at one column.
+__device__ __forceinline__ void chain_value(const float (&vv)[4], float pre, float diffx, float diffy,
+                                            float &ox, float &oy)
+{
+    const float dh = vv[1] - vv[0];
+    const float dv = vv[3] - vv[2];
+    const float X = (-diffy) * (-dh) - (-diffx) * (-dv);
+    ox = ((-pre) * (-diffy)) * X;
+    oy = (pre * (-diffx)) * X;
+}
+
+__global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
 {
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
@@ -1221,11 +1283,9 @@ __global__ void __launch_bounds__(NE_THREADS, 3) k_normal_eq(DModel m, DBatch b)
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
     extern __shared__ __align__(16) double nesm[];
     const int KTP = m.KTP, KT = m.KT;
-    double *rows = nesm;                         // [2*NE_SUB][KTP]
-    double *wts = rows + 2 * NE_SUB * KTP;       // [2*NE_SUB]
-    __shared__ int s_nb[4][NE_SUB];              // kl, kr, ka, kb
-    __shared__ float s_pre[NE_SUB], s_dx[NE_SUB], s_dy[NE_SUB];
+    __shared__ ChunkHead hd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int a_low = lane & 7, q_me = 4 * warp + (lane >> 3);
     const int nb4 = KTP / 4;
     int bi, bj;
     ne_block(tid, nb4, bi, bj);
@@ -1242,68 +1302,33 @@ __global__ void __launch_bounds__(NE_THREADS, 3) k_normal_eq(DModel m, DBatch b)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
         double gacc = 0.0;
-        const int c0 = ch * NE_CH, c1 = min(N, c0 + NE_CH);
-        for (int n0 = c0; n0 < c1; n0 += NE_SUB) {
-            const int cn = min(NE_SUB, c1 - n0);
-            // per-fragment scalars and neighbour indices
-            if (tid < NE_SUB) {
-                const int q = tid, n = n0 + q;
-                float pre = 0.0f, dx = 0.0f, dy = 0.0f, wx = 0.0f, wy = 0.0f;
-                int k0 = 0, k1 = 0, k2 = 0, k3 = 0;
-                if (q < cn) {
-                    const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
-                    pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
-                    dx = 2 * gx;
-                    dy = 2 * gy;
-                    wx = fg[3 * NMAX + n];
-                    wy = fg[4 * NMAX + n];
-                    k0 = nb[n]; k1 = nb[NMAX + n]; k2 = nb[2 * NMAX + n]; k3 = nb[3 * NMAX + n];
-                }
-                s_pre[q] = pre; s_dx[q] = dx; s_dy[q] = dy;
-                s_nb[0][q] = k0; s_nb[1][q] = k1; s_nb[2][q] = k2; s_nb[3][q] = k3;
-                wts[2 * q] = (double)wx;
-                wts[2 * q + 1] = (double)wy;
-            }
-            __syncthreads();
-            // rows: warp w builds fragments w, w+8, w+16, w+24, lanes take columns; the four
-            // neighbour rows of two fragments are loaded before any is used
-            for (int cb = 0; cb < KTP; cb += 96)
+        const int c0 = ch * NE_CH, cnt = min(N, c0 + NE_CH) - c0;
+        const int nsub = (cnt + NE_SUB - 1) / NE_SUB;
+        __syncthreads();                          // the previous chunk is done with hd
+        chunk_head(hd, fg, nb, c0, cnt);
+        __syncthreads();
+        float v[NE_GRP][4];
+        chunk_prefetch<NE_GRP>(v, hd, Jf, KT, KTP, q_me, cnt, a_low);
+        for (int it = 0; it < nsub; ++it) {
+            // rows of stage it (double buffered: the other buffer is being summed)
+            double *rows = nesm + (size_t)(it & 1) * 2 * NE_SUB * KTP;      // [2*NE_SUB][KTP]
+            {
+                const int ql = q_me, q = it * NE_SUB + ql;
+                const float pre = hd.pre[q], diffx = hd.dx[q], diffy = hd.dy[q];
+                const bool live = q < cnt;
 #pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                float v[2][3][4];
-#pragma unroll
-                for (int i = 0; i < 2; ++i) {
-                    const int q = warp + 8 * (2 * half + i);
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const int j = cb + lane + 32 * c;
-#pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            v[i][c][r] = (q < cn && j < KT) ? Jf[(size_t)s_nb[r][q] * KTP + j] : 0.0f;
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < 2; ++i) {
-                    const int q = warp + 8 * (2 * half + i);
-                    const float pre = s_pre[q], diffx = s_dx[q], diffy = s_dy[q];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const int j = cb + lane + 32 * c;
-                        if (j >= KTP) continue;
-                        float ox = 0.0f, oy = 0.0f;
-                        if (q < cn && j < KT) {
-                            const float dh = v[i][c][1] - v[i][c][0];
-                            const float dv = v[i][c][3] - v[i][c][2];
-                            const float X = (-diffy) * (-dh) - (-diffx) * (-dv);
-                            ox = ((-pre) * (-diffy)) * X;
-                            oy = (pre * (-diffx)) * X;
-                        }
-                        rows[(2 * q) * KTP + j] = (double)ox;
-                        rows[(2 * q + 1) * KTP + j] = (double)oy;
-                    }
+                for (int g = 0; g < NE_GRP; ++g) {
+                    const int a = 8 * g + a_low;
+                    if (a >= KTP) continue;
+                    float ox = 0.0f, oy = 0.0f;
+                    if (live && a < KT) chain_value(v[g], pre, diffx, diffy, ox, oy);
+                    rows[(2 * ql) * KTP + a] = (double)ox;
+                    rows[(2 * ql + 1) * KTP + a] = (double)oy;
                 }
             }
             __syncthreads();
+            if (it + 1 < nsub) chunk_prefetch<NE_GRP>(v, hd, Jf, KT, KTP, (it + 1) * NE_SUB + q_me, cnt, a_low);
+            const int cn = min(NE_SUB, cnt - it * NE_SUB);
             if (bi >= 0) {
                 for (int q = 0; q < cn; ++q) {
                     const double *rx = rows + (2 * q) * KTP, *ry = rx + KTP;
@@ -1324,10 +1349,11 @@ __global__ void __launch_bounds__(NE_THREADS, 3) k_normal_eq(DModel m, DBatch b)
                 }
             }
             if (tid < KTP) {
-                for (int q = 0; q < cn; ++q)
-                    gacc = fma(wts[2 * q + 1], rows[(2 * q + 1) * KTP + tid], fma(wts[2 * q], rows[(2 * q) * KTP + tid], gacc));
+                for (int q = 0; q < cn; ++q) {
+                    const int qc = it * NE_SUB + q;
+                    gacc = fma(hd.w[2 * qc + 1], rows[(2 * q + 1) * KTP + tid], fma(hd.w[2 * qc], rows[(2 * q) * KTP + tid], gacc));
+                }
             }
-            __syncthreads();
         }
         double *part = b.ne_part + ((size_t)f * NE_MAXCH + ch) * stride;
         if (bi >= 0) {
@@ -1744,7 +1770,10 @@ __global__ void __launch_bounds__(1024) k_compact_active(DBatch b, int *out)
         if (tid == 1023) s_base += s_warp[31] + __popc(mask);
         __syncthreads();
     }
-    if (tid == 0) *out = s_base;
+    if (tid == 0) {
+        out[0] = s_base;
+        out[1] = *b.err;
+    }
 }
 
 }  // namespace tdi

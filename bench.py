@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-frames", type=int, default=8, help="frames of the CPU sample")
     ap.add_argument("--profile-kernel", default="raster")
     ap.add_argument("--plain-frames", type=int, default=16, help="frames of the unbatched (plain) run")
+    ap.add_argument("--normal-eq", default="exact", choices=["exact", "tensor"],
+                    help="normal equations: FP64 in the oracle's order, or split-BF16 on the tensor cores")
     return ap.parse_args()
 
 
@@ -221,7 +223,8 @@ def main():
     fr.target = synth.add_noise(img, 0.02, 3 + rank)
     batch.set_frames(fr)
     lam0 = np.tile(synth.LAMBDA_INIT, (F, 1)).astype(np.float32)
-    cfg = tdi.default_config(max_iters_rigid=MAX_ITERS)
+    cfg = tdi.default_config(max_iters_rigid=MAX_ITERS,
+                             normal_eq=tdi.NORMAL_EQ_TENSOR if args.normal_eq == "tensor" else tdi.NORMAL_EQ_EXACT)
 
     def barrier():
         if world > 1:
@@ -319,7 +322,8 @@ def main():
                    "max_outer_iters": MAX_ITERS, "crop": "256x256",
                    "mean_fragments": n_frag,
                    "l2": "inputs larger than L2 (256 MB of crops per 1,024 frames)",
-                   "parallelism": f"frames sharded over {world} GPU(s), no collective"},
+                   "parallelism": f"frames sharded over {world} GPU(s), no collective",
+                   "normal_eq": args.normal_eq},
         "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),

@@ -85,6 +85,12 @@ typedef struct {
     int32_t max_iters_lambda;    /* outer iterations of the light fit (10000) */
     float ref_face_size;         /* REF_FACE_SIZE */
     float taps[15];              /* Gaussian taps for KERNEL_SIGMA (video_fitter.cu:53-61) */
+    int32_t normal_eq;           /* normal equations J^T J, J^T r (derivative_computer.cu:157-163):
+                                  * 0 = FP64 sums in the oracle's fixed order (bit-exact);
+                                  * 1 = split-BF16 products on the tensor cores, FP32
+                                  *     accumulation per 256-fragment chunk (g stays exact).
+                                  *     No counterpart in the reference (which uses
+                                  *     cublasSgemm). */
 } tdi_fit_config;
 
 typedef struct {

@@ -141,3 +141,40 @@ def test_raster_stays_exact_across_the_depth_key_epoch_wrap(tdi, synth, O, small
             assert np.array_equal(got["tri"], ref["tri"]), it
             assert np.array_equal(got["owner"], ref["owner"]), it
             assert np.array_equal(got["pix"], ref["pix"]), it
+
+
+@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+def test_tensor_core_normal_equations_within_fp32_accumulation_error(request, tdi, synth, O, case_name):
+    """normal_eq = 1: J^T J and J^T r from split-BF16 products on the tensor cores, FP32
+    accumulation per 256-fragment chunk. Against the oracle's FP64 sums: relative error of H
+    (Frobenius) and of g (max norm) within 1e-5, the class of the reference's own cublasSgemm."""
+    case = request.getfixturevalue(case_name)
+    m, fr, om = case
+    model, batch, lam, L = _setup(tdi, case, synth)
+    cfg = tdi.default_config(normal_eq=tdi.NORMAL_EQ_TENSOR)
+    fs = O.FrameSet(fr)
+    batch.set_state(fr.state_init, lam, L)
+    batch.evaluate(cfg)
+    for i in range(fr.n_frames):
+        e = O.evaluate(om, fs, i, O.config(), fr.state_init[i], lam[i], float(L[i]))
+        ne = batch.read(i, tdi.READ_NORMAL_EQ)
+        H, Ho = ne["H"].astype(np.float64), e["H"].astype(np.float64)
+        assert np.array_equal(H, H.T)
+        assert np.linalg.norm(H - Ho) <= 1e-5 * np.linalg.norm(Ho)
+        assert np.abs(ne["g"] - e["g"]).max() <= 1e-5 * np.abs(e["g"]).max()
+        # everything upstream of the normal equations is unchanged
+        assert np.array_equal(_bits(batch.read(i, tdi.READ_JACOBIAN)), _bits(e["J"]))
+
+
+def test_tensor_core_fit_reaches_the_exact_fits_objective(tdi, synth, O, small_case):
+    """Fits with tensor-core normal equations follow different (rounding-level) search
+    directions, so their iterates are not the oracle's; they must end at an objective within
+    0.5% of the exact fit's, with the same status flags."""
+    m, fr, om = small_case
+    model, batch, lam, L = _setup(tdi, small_case, synth)
+    x0, lam0, rep0 = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(max_iters_rigid=10))
+    x1, lam1, rep1 = batch.fit_frames(fr, fr.state_init, lam, L,
+                                      tdi.default_config(max_iters_rigid=10, normal_eq=tdi.NORMAL_EQ_TENSOR))
+    for i in range(fr.n_frames):
+        assert rep1[i].flags == rep0[i].flags
+        assert abs(rep1[i].objective - rep0[i].objective) <= 5e-3 * abs(rep0[i].objective)
