@@ -242,7 +242,7 @@ struct Launch {
     const DBatch &b;
     cudaStream_t s;
     int F;
-    size_t smem_vertex() const { return (size_t)(3 * m.KP * 33 + VT_F * m.KP) * sizeof(float); }
+    size_t smem_vertex() const { return (size_t)(3 * m.KP * VT_PITCH + VT_F * m.KP + VT_F * VT_FR) * sizeof(float); }
     size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
     size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * m.KTP * sizeof(double); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }

@@ -167,99 +167,136 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 
 // ------------------------------------------------------------------------------------------
 // Vertex stage: X0 = mean + E*eps (sequential fmaf over k), camera transform and
-// projection (renderer.cu:806-861, funcs.cu:395-453) for a tile of 32 vertices x 32 frames.
-// geo[f] = [X0 | Y0 | Z0] planes of V floats; proj[f][v] = (xp, yp, camera Z, 0).
+// projection (renderer.cu:806-861, funcs.cu:395-453) for a tile of VT_V vertices x 64 frames:
+// a thread owns VT_VPT vertices (tx + 32*h) x 8 frames; the basis rows of the tile and the
+// frames' coefficients, rotations, translations, cameras and render flags are staged in
+// shared memory. geo[f] = [X0 | Y0 | Z0] planes of V floats (vertex slots);
+// proj[f][slot] = (xp, yp, camera Z, 0).
 
-constexpr int VT_V = 32, VT_FPT = 8, VT_F = 8 * VT_FPT;   // vertices, frames per block; frames per thread
+constexpr int VT_VPT = 1, VT_V = 32 * VT_VPT;             // vertices per thread, per block
+constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
+constexpr int VT_PITCH = VT_V + 1;                          // basis row pitch in shared memory
+constexpr int VT_FR = 16;                                   // per-frame floats: R(9), tau(3), cam(4)
 
 __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
 {
     extern __shared__ float vsm[];
     const int KP = m.KP, K = m.K;
-    float *Es = vsm;                           // [3*KP][33]: basis rows, vertex-minor
-    float *Xs = vsm + 3 * KP * 33;             // [VT_F][KP]: coefficients per frame
+    float *Es = vsm;                           // [3*KP][VT_PITCH]: basis rows, vertex-minor
+    float *Xs = Es + 3 * KP * VT_PITCH;        // [VT_F][KP]: coefficients per frame
+    float *Fs = Xs + VT_F * KP;                // [VT_F][VT_FR]
     __shared__ int s_any;
+    __shared__ int s_render[VT_F], s_frame[VT_F];
     // frame tiles vary fastest, so the blocks that share a basis tile run together and read
     // it from L2
     const int v0 = blockIdx.y * VT_V, f0 = blockIdx.x * VT_F;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     if (tid == 0) s_any = 0;
     __syncthreads();
-    if (tid < VT_F && f0 + tid < b.nact && b.ctl[b.act[f0 + tid]].render) {
-        s_any = 1;
-        if (blockIdx.y == 0) prof_count(b, KID_VERTEX);
+    if (tid < VT_F) {
+        const int ai = f0 + tid;
+        const int f = ai < b.nact ? b.act[ai] : -1;
+        const int r = f >= 0 && b.ctl[f].render;
+        s_frame[tid] = f;
+        s_render[tid] = r;
+        if (r) {
+            s_any = 1;
+            if (blockIdx.y == 0) prof_count(b, KID_VERTEX);
+        }
     }
     __syncthreads();
     if (!s_any) return;
     const int nv = min(VT_V, m.V - v0);
     for (int vl = threadIdx.y; vl < VT_V; vl += 8) {
         const float *er = m.E + (size_t)(v0 + vl) * 3 * KP;
-        for (int rem = threadIdx.x; rem < 3 * KP; rem += 32) Es[rem * 33 + vl] = vl < nv ? er[rem] : 0.0f;
+        for (int rem = threadIdx.x; rem < 3 * KP; rem += 32) Es[rem * VT_PITCH + vl] = vl < nv ? er[rem] : 0.0f;
     }
     for (int fl = threadIdx.y; fl < VT_F; fl += 8) {
-        const int ai = f0 + fl;
-        const float *xr = ai < b.nact ? b.xe + (size_t)b.act[ai] * m.KTP : nullptr;
+        const int f = s_frame[fl];
+        const float *xr = f >= 0 ? b.xe + (size_t)f * m.KTP : nullptr;
         for (int k = threadIdx.x; k < KP; k += 32) Xs[fl * KP + k] = (xr && k < K) ? xr[k] : 0.0f;
+        if (threadIdx.x < VT_FR) {
+            const int i = threadIdx.x;
+            float v = 0.0f;
+            if (f >= 0) v = i < 9 ? b.R[f * 9 + i] : i < 12 ? b.xe[(size_t)f * m.KTP + K + (i - 9)] : b.cam[f * 4 + (i - 12)];
+            Fs[fl * VT_FR + i] = v;
+        }
     }
     __syncthreads();
     const int vl = threadIdx.x;
-    const int v = v0 + vl;
-    float acc[VT_FPT][3];
+    float acc[VT_FPT][VT_VPT][3];
 #pragma unroll
-    for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
+    for (int q = 0; q < VT_FPT; ++q)
+#pragma unroll
+        for (int h = 0; h < VT_VPT; ++h) acc[q][h][0] = acc[q][h][1] = acc[q][h][2] = 0.0f;
     const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
+    const float *e0p = Es + vl, *e1p = Es + KP * VT_PITCH + vl, *e2p = Es + 2 * KP * VT_PITCH + vl;
     // sequential fused multiply-add over k for every output (the order the oracle uses)
     int k = 0;
     for (; k + 4 <= K; k += 4) {
-        float e[3][4];
+        float e[3][4][VT_VPT];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) e[c][j] = Es[(c * KP + k + j) * 33 + vl];
+            for (int h = 0; h < VT_VPT; ++h) {
+                e[0][j][h] = e0p[(k + j) * VT_PITCH + 32 * h];
+                e[1][j][h] = e1p[(k + j) * VT_PITCH + 32 * h];
+                e[2][j][h] = e2p[(k + j) * VT_PITCH + 32 * h];
+            }
 #pragma unroll
         for (int q = 0; q < VT_FPT; ++q) {
             const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
             const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                acc[q][0] = fmaf(e[0][j], xv[j], acc[q][0]);
-                acc[q][1] = fmaf(e[1][j], xv[j], acc[q][1]);
-                acc[q][2] = fmaf(e[2][j], xv[j], acc[q][2]);
-            }
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int h = 0; h < VT_VPT; ++h) {
+                    acc[q][h][0] = fmaf(e[0][j][h], xv[j], acc[q][h][0]);
+                    acc[q][h][1] = fmaf(e[1][j][h], xv[j], acc[q][h][1]);
+                    acc[q][h][2] = fmaf(e[2][j][h], xv[j], acc[q][h][2]);
+                }
         }
     }
     for (; k < K; ++k) {
-        const float ex = Es[(0 * KP + k) * 33 + vl];
-        const float ey = Es[(1 * KP + k) * 33 + vl];
-        const float ez = Es[(2 * KP + k) * 33 + vl];
+        float e[3][VT_VPT];
+#pragma unroll
+        for (int h = 0; h < VT_VPT; ++h) {
+            e[0][h] = e0p[k * VT_PITCH + 32 * h];
+            e[1][h] = e1p[k * VT_PITCH + 32 * h];
+            e[2][h] = e2p[k * VT_PITCH + 32 * h];
+        }
 #pragma unroll
         for (int q = 0; q < VT_FPT; ++q) {
-            const float e = xr[q * KP + k];
-            acc[q][0] = fmaf(ex, e, acc[q][0]);
-            acc[q][1] = fmaf(ey, e, acc[q][1]);
-            acc[q][2] = fmaf(ez, e, acc[q][2]);
+            const float xv = xr[q * KP + k];
+#pragma unroll
+            for (int h = 0; h < VT_VPT; ++h) {
+                acc[q][h][0] = fmaf(e[0][h], xv, acc[q][h][0]);
+                acc[q][h][1] = fmaf(e[1][h], xv, acc[q][h][1]);
+                acc[q][h][2] = fmaf(e[2][h], xv, acc[q][h][2]);
+            }
         }
     }
-    if (v >= m.V) return;
-    const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
 #pragma unroll
-    for (int q = 0; q < VT_FPT; ++q) {
-        const int ai = f0 + threadIdx.y * VT_FPT + q;
-        if (ai >= b.nact) continue;
-        const int f = b.act[ai];
-        if (!b.ctl[f].render) continue;
-        const float *R = b.R + f * 9;
-        const float *tau = b.xe + (size_t)f * m.KTP + K;
-        const float *cam = b.cam + f * 4;
-        const float X0 = mx + acc[q][0], Y0 = my + acc[q][1], Z0 = mz + acc[q][2];
-        const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
-        const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
-        const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
-        float *g = b.geo + (size_t)f * 6 * m.V;
-        g[v] = X0;
-        g[m.V + v] = Y0;
-        g[2 * m.V + v] = Z0;
-        b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
+    for (int h = 0; h < VT_VPT; ++h) {
+        const int v = v0 + vl + 32 * h;
+        if (v >= m.V) continue;
+        const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
+#pragma unroll
+        for (int q = 0; q < VT_FPT; ++q) {
+            const int fl = threadIdx.y * VT_FPT + q;
+            if (!s_render[fl]) continue;
+            const int f = s_frame[fl];
+            const float *R = Fs + fl * VT_FR, *tau = R + 9, *cam = R + 12;
+            const float X0 = mx + acc[q][h][0], Y0 = my + acc[q][h][1], Z0 = mz + acc[q][h][2];
+            const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
+            const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
+            const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
+            float *g = b.geo + (size_t)f * 6 * m.V;
+            g[v] = X0;
+            g[m.V + v] = Y0;
+            g[2 * m.V + v] = Z0;
+            b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
+        }
     }
 }
 

@@ -36,6 +36,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "cap53k_video"
 MAX_ITERS = 20
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 METRIC = "fitted frames/s (batched video fit, 53,490-vertex model, 256x256 crop)"
 
 
@@ -47,7 +48,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=1024, help="frames per GPU per step")
     ap.add_argument("--cpu-frames", type=int, default=8, help="frames of the CPU sample")
-    ap.add_argument("--profile-kernel", default="raster")
+    ap.add_argument("--profile-kernel", default="vertex",
+                    help="kernel timed live for the roofline (the largest share of the step)")
     ap.add_argument("--plain-frames", type=int, default=16, help="frames of the unbatched (plain) run")
     ap.add_argument("--normal-eq", default="exact", choices=["exact", "tensor"],
                     help="normal equations: FP64 in the oracle's order, or split-BF16 on the tensor cores")
@@ -124,21 +126,28 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-def algorithmic_bytes_per_frame(kernel: str, V: int, T: int, K: int, n_frag: float) -> float:
-    """Bytes a kernel must move per frame it processes (what the roofline divides by)."""
-    if kernel == "raster":
-        # projected vertices (xp, yp, Z) + triangle indices + the fragment list written
-        return 3 * V * 4 + 3 * T * 4 + n_frag * 16
+def algorithmic_bytes(kernel: str, V: int, T: int, K: int, n_frag: float):
+    """(bytes per frame, bytes per launch) a kernel must move: what the roofline divides by."""
     if kernel == "vertex":
-        # output planes per frame; the basis (3*V*K*4) is shared across the launch's frames
-        return 6 * V * 4 + K * 4
+        # outputs per frame (object coordinates 12 B, projection 16 B per vertex) and the
+        # coefficients; the basis (3*V*K*4 B) once per launch, shared by all its frames
+        return 28.0 * V + 4.0 * K, 12.0 * V * K
+    if kernel == "raster":
+        # depth pass: projections (16 B per vertex), triangle corners and visiting order
+        # (16 B per triangle), one 8-byte depth key per visible fragment
+        return 16.0 * V + 16.0 * T + 8.0 * n_frag, 0.0
     if kernel == "render":
         # fragments, three vertices' object coordinates and albedo, four target pixels, gradients
-        return n_frag * (16 + 3 * 16 + 4 * 4 + 5 * 4)
+        return n_frag * (16 + 3 * 16 + 4 * 4 + 5 * 4), 0.0
     if kernel == "jacobian":
         # three vertices' basis rows (3 coords x K) and the row written
-        return n_frag * (3 * 3 * K * 4 + (K + 6) * 4)
+        return n_frag * (3 * 3 * K * 4 + (K + 6) * 4), 0.0
     raise ValueError(kernel)
+
+
+def vertex_flops_per_frame(V: int, K: int) -> float:
+    """Fused multiply-adds of the basis x coefficient products, 2 flops each."""
+    return 2.0 * 3 * V * K
 
 
 def cpu_fit_rate(O, synth, m, fr, n_frames, threads):
@@ -287,30 +296,51 @@ def main():
         if st != 0:
             raise tdi.TdiError(lib.tdi_last_error().decode())
         e2e_ms += e0.elapsed_time(e1)
+    # the other normal-equation mode on the same batch, device-resident, same step count
+    other = "tensor" if args.normal_eq == "exact" else "exact"
+    cfg_o = tdi.default_config(max_iters_rigid=MAX_ITERS,
+                               normal_eq=tdi.NORMAL_EQ_TENSOR if other == "tensor" else tdi.NORMAL_EQ_EXACT)
+    batch.set_state(fr.state_init, lam0, L)
+    batch.fit(cfg_o)
+    other_ms = 0.0
+    for _ in range(args.steps):
+        batch.set_state(fr.state_init, lam0, L)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.fit(cfg_o)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        other_ms += e0.elapsed_time(e1)
+    xo_gpu, _, rep_o = batch.get_state()
     h2d = sum(h[k].numel() * h[k].element_size() for k in ("t", "xl", "yl", "b", "fs", "cam", "o", "x", "lam", "L"))
     d2h = F * (m.n_expr + 6) * 4 + F * 3 * 4 + F * C.sizeof(tdi.Report)
 
     # max over ranks
-    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([total_ms, e2e_ms, other_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms = t.tolist()
+    total_ms, e2e_ms, other_ms = t.tolist()
     frames_all = F * world * args.steps
     value = frames_all / (total_ms / 1000.0)
     e2e = frames_all / (e2e_ms / 1000.0)
 
     hbm, tfl, peak_kind = measured_peaks()
-    per_frame = algorithmic_bytes_per_frame(args.profile_kernel, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
+    per_frame, per_launch = algorithmic_bytes(args.profile_kernel, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
     avg_launch_s = prof_ms / 1000.0 / max(prof_launches, 1)
     frames_per_launch = prof_frames / max(prof_launches, 1)
-    achieved = per_frame * frames_per_launch / avg_launch_s / 1e9 if prof_launches else None
+    bytes_per_launch = per_frame * frames_per_launch + per_launch
+    achieved = bytes_per_launch / avg_launch_s / 1e9 if prof_launches else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tr = json.load(f).get(args.profile_kernel)
         if tr:
-            traffic = tr["dram_bytes_per_frame"] * frames_per_launch
+            traffic = tr["dram_bytes_per_frame"] * frames_per_launch + tr.get("dram_bytes_per_launch", 0.0)
 
     line = {
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
@@ -332,7 +362,21 @@ def main():
                      "frac": achieved / hbm if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "launches": prof_launches,
                      "avg_launch_ms": avg_launch_s * 1000.0, "frames_per_launch": frames_per_launch,
-                     "algorithmic_bytes_per_frame": per_frame},
+                     "algorithmic_bytes_per_frame": per_frame, "algorithmic_bytes_per_launch": per_launch},
+        "compute": ({"kernel": "vertex", "achieved": vertex_flops_per_frame(m.n_vertices, m.n_expr) * frames_per_launch
+                                                     / avg_launch_s / 1e12,
+                     "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                     "frac": vertex_flops_per_frame(m.n_vertices, m.n_expr) * frames_per_launch / avg_launch_s / 1e12
+                             / FP32_NOMINAL_TFLOPS,
+                     "peak_source": "nominal FP32 SIMT: 148 SMs x 128 lanes x 2 flops x 1.965 GHz",
+                     "note": "basis x coefficients as a sequential FP32 FMA chain (bit-exact order), no tensor-core form"}
+                    if args.profile_kernel == "vertex" and prof_launches else None),
+        "normal_eq_modes": {args.normal_eq: {"value": value, "ms_per_step": total_ms / args.steps},
+                            other: {"value": frames_all / (other_ms / 1000.0), "ms_per_step": other_ms / args.steps,
+                                    "mean_renders": float(np.mean([r.renders for r in rep_o])),
+                                    "failed": int(sum(1 for r in rep_o if r.flags & tdi.FLAG_FAIL))},
+                            "note": "exact: FP64 normal equations in the oracle's order (bit-identical fits); "
+                                    "tensor: split-BF16 tcgen05 products, FP32 chunk accumulation"},
         "clocks": clk,
         "fit": {"mean_iters_rigid": float(np.mean([r.iters_rigid for r in rep])),
                 "mean_iters_lambda": float(np.mean([r.iters_lambda for r in rep])),
@@ -374,13 +418,15 @@ def main():
             om = O.Model(m)
             fs = O.FrameSet(fr, 0, n)
             ocfg = O.config(max_iters_rigid=MAX_ITERS)
-            errs = {}
+            errs = {args.normal_eq: {}, other: {}}
             for kind in ("f32", "f64"):
                 ox, ol, orep = O.fit_frames(om, fs, ocfg, fr.state_init[:n], lam0[:n], L[:n], kind=kind)
-                rel = np.abs(x[:n] - ox) / np.maximum(np.abs(ox), 1e-2)
-                errs[kind] = {"max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
-                              "frames_within_1e-5": int(np.sum(rel.max(axis=1) <= 1e-5))}
-            line["param_err"] = {"frames": n, "vs_fp32_oracle": errs["f32"], "vs_fp64_oracle": errs["f64"],
+                for mode, xg in ((args.normal_eq, x), (other, xo_gpu)):
+                    rel = np.abs(xg[:n] - ox) / np.maximum(np.abs(ox), 1e-2)
+                    errs[mode]["vs_" + ("fp32" if kind == "f32" else "fp64") + "_oracle"] = {
+                        "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+                        "frames_within_1e-5": int(np.sum(rel.max(axis=1) <= 1e-5))}
+            line["param_err"] = {"frames": n, **errs[args.normal_eq], other: errs[other],
                                  "definition": "|x_gpu - x_oracle| / max(|x_oracle|, 1e-2) over pose and expressions"}
     if rank == 0:
         print(json.dumps(line), flush=True)
