@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libtdi_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "tdi_api.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("tdi_kernels.cu", "tdi_internal.cuh", "tdi_noalloc.cu", "tdi_normal_tc.cu")] + [
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("tdi_kernels.cu", "tdi_internal.cuh", "tdi_noalloc.cu", "tdi_normal_tc.cu", "tdi_async.cuh")] + [
     os.path.join(HERE, "..", "include", "tdi.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

@@ -236,13 +236,28 @@ tdi_status set_attrs()
     return TDI_OK;
 }
 
+// Vertex stage grid: frame tiles x vertex-tile groups, about VT_BLOCKS_PER_SM blocks per SM.
+dim3 vertex_grid(const DModel &m, int frames)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    const int ftiles = (frames + VT_F - 1) / VT_F;
+    const int ntiles = (m.V + VT_V - 1) / VT_V;
+    const int groups = std::max(1, std::min(ntiles, VT_BLOCKS_PER_SM * sms / std::max(ftiles, 1)));
+    return dim3(std::max(ftiles, 1), groups);
+}
+
 struct Launch {
     tdi_batch *bt;
     const DModel &m;
     const DBatch &b;
     cudaStream_t s;
     int F;
-    size_t smem_vertex() const { return (size_t)(3 * m.KP * VT_PITCH + VT_F * m.KP + VT_F * VT_FR) * sizeof(float); }
+    size_t smem_vertex() const { return vt_smem(m.KP); }
     size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
     size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * m.KTP * sizeof(double); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
@@ -259,7 +274,7 @@ tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
     TDI_TRY(launch(bt, 0, k_compact_active, dim3(1), dim3(1024), 0, s, (const DBatch)bt->d, bt->d_count));
     TDI_CUDA(cudaMemcpyAsync(bt->h_count, bt->d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     TDI_CUDA(cudaStreamSynchronize(s));
-    if (bt->h_count[1]) return fail(TDI_ERR_CUDA, "a tensor-core wait in the normal equations gave up");
+    if (bt->h_count[1]) return fail(TDI_ERR_CUDA, "a bounded device-side wait gave up (error word set)");
     *n = *bt->h_count;
     bt->d.nact = *n;
     return TDI_OK;
@@ -267,8 +282,7 @@ tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
 
 tdi_status geometry(const Launch &L, const Cfg &c, int stage)
 {
-    dim3 vg((L.A() + VT_F - 1) / VT_F, (L.m.V + VT_V - 1) / VT_V);
-    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
                    (size_t)PC_WARPS * (2 * L.m.K + 4 * NL) * sizeof(float), L.s, L.m, L.b, c, stage));
     TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
@@ -792,8 +806,7 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     TDI_TRY(compact_active(b, s, &n));
     if (n > 0) {
         TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
-        dim3 vg((n + VT_F - 1) / VT_F, (m.V + VT_V - 1) / VT_V);
-        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vg, dim3(32, 8), L.smem_vertex(), s, m, d));
+        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, 8), L.smem_vertex(), s, m, d));
         TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, n), dim3(RD_THREADS), 0, s, m, d));
         TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));
     }

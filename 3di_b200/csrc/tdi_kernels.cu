@@ -2,6 +2,7 @@
 // below is evaluated in the operand order of the 3DI sources it restates, without FMA
 // contraction, so each per-fragment quantity is bit-identical to the CPU oracle's.
 #include "tdi_internal.cuh"
+#include "tdi_async.cuh"
 
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
@@ -167,29 +168,36 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 
 // ------------------------------------------------------------------------------------------
 // Vertex stage: X0 = mean + E*eps (sequential fmaf over k), camera transform and
-// projection (renderer.cu:806-861, funcs.cu:395-453) for a tile of VT_V vertices x 64 frames:
-// a thread owns VT_VPT vertices (tx + 32*h) x 8 frames; the basis rows of the tile and the
-// frames' coefficients, rotations, translations, cameras and render flags are staged in
-// shared memory. geo[f] = [X0 | Y0 | Z0] planes of V floats (vertex slots);
-// proj[f][slot] = (xp, yp, camera Z, 0).
+// projection (renderer.cu:806-861, funcs.cu:395-453). A block owns 64 frames (coefficients,
+// rotations, translations, cameras and render flags staged in shared memory) and walks a
+// strided set of 32-vertex tiles; each tile's basis rows (32 x 3 x KP floats, contiguous in
+// HBM) are brought into shared memory by the TMA engine, one bulk copy per vertex row,
+// double-buffered so that the next tile streams in while this one is computed. A thread
+// owns one vertex x 8 frames (24 FMA chains). geo[f] = [X0 | Y0 | Z0] planes of V floats
+// (vertex slots); proj[f][slot] = (xp, yp, camera Z, 0).
 
-constexpr int VT_VPT = 1, VT_V = 32 * VT_VPT;             // vertices per thread, per block
+constexpr int VT_V = 32;                                   // vertices per tile (one per lane)
 constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
-constexpr int VT_PITCH = VT_V + 1;                          // basis row pitch in shared memory
 constexpr int VT_FR = 16;                                   // per-frame floats: R(9), tau(3), cam(4)
+constexpr int VT_BLOCKS_PER_SM = 2;
 
-__global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
+__host__ __device__ __forceinline__ int vt_row(int KP) { return 3 * KP + 4; }   // basis row pitch (floats)
+__host__ __device__ __forceinline__ size_t vt_smem(int KP)
 {
-    extern __shared__ float vsm[];
-    const int KP = m.KP, K = m.K;
-    float *Es = vsm;                           // [3*KP][VT_PITCH]: basis rows, vertex-minor
-    float *Xs = Es + 3 * KP * VT_PITCH;        // [VT_F][KP]: coefficients per frame
+    return ((size_t)2 * VT_V * vt_row(KP) + (size_t)VT_F * KP + (size_t)VT_F * VT_FR) * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBatch b)
+{
+    extern __shared__ __align__(16) float vsm[];
+    const int KP = m.KP, K = m.K, ER = vt_row(KP);
+    float *Eb = vsm;                           // [2][VT_V][ER]: basis rows of two tiles
+    float *Xs = Eb + 2 * VT_V * ER;            // [VT_F][KP]: coefficients per frame
     float *Fs = Xs + VT_F * KP;                // [VT_F][VT_FR]
     __shared__ int s_any;
     __shared__ int s_render[VT_F], s_frame[VT_F];
-    // frame tiles vary fastest, so the blocks that share a basis tile run together and read
-    // it from L2
-    const int v0 = blockIdx.y * VT_V, f0 = blockIdx.x * VT_F;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    const int f0 = blockIdx.x * VT_F;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     if (tid == 0) s_any = 0;
     __syncthreads();
@@ -206,10 +214,25 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
     }
     __syncthreads();
     if (!s_any) return;
-    const int nv = min(VT_V, m.V - v0);
-    for (int vl = threadIdx.y; vl < VT_V; vl += 8) {
-        const float *er = m.E + (size_t)(v0 + vl) * 3 * KP;
-        for (int rem = threadIdx.x; rem < 3 * KP; rem += 32) Es[rem * VT_PITCH + vl] = vl < nv ? er[rem] : 0.0f;
+    const int ntiles = (m.V + VT_V - 1) / VT_V;
+    const int rowbytes = 3 * KP * (int)sizeof(float);
+    const uint32_t eb_addr = smem_addr(Eb);
+    auto issue = [&](int j) {                  // thread 0: tile j of this block into buffer j & 1
+        const int t = blockIdx.y + j * gridDim.y;
+        if (t >= ntiles) return;
+        const int nv = min(VT_V, m.V - t * VT_V), buf = j & 1;
+        const uint32_t bar = smem_addr(&s_bar[buf]);
+        mbar_expect_tx(bar, (uint32_t)(nv * rowbytes));
+        for (int r = 0; r < nv; ++r)
+            bulk_g2s(eb_addr + (uint32_t)((buf * VT_V + r) * ER) * 4u, m.E + (size_t)(t * VT_V + r) * 3 * KP,
+                     (uint32_t)rowbytes, bar);
+    };
+    if (tid == 0) {
+        mbar_init(smem_addr(&s_bar[0]), 1);
+        mbar_init(smem_addr(&s_bar[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue(0);
+        issue(1);
     }
     for (int fl = threadIdx.y; fl < VT_F; fl += 8) {
         const int f = s_frame[fl];
@@ -224,79 +247,82 @@ __global__ void __launch_bounds__(256) k_vertex(DModel m, DBatch b)
     }
     __syncthreads();
     const int vl = threadIdx.x;
-    float acc[VT_FPT][VT_VPT][3];
-#pragma unroll
-    for (int q = 0; q < VT_FPT; ++q)
-#pragma unroll
-        for (int h = 0; h < VT_VPT; ++h) acc[q][h][0] = acc[q][h][1] = acc[q][h][2] = 0.0f;
     const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
-    const float *e0p = Es + vl, *e1p = Es + KP * VT_PITCH + vl, *e2p = Es + 2 * KP * VT_PITCH + vl;
-    // sequential fused multiply-add over k for every output (the order the oracle uses)
-    int k = 0;
-    for (; k + 4 <= K; k += 4) {
-        float e[3][4][VT_VPT];
+    int j = 0;
+    bool ok = true;
+    for (;; ++j) {
+        const int t = blockIdx.y + j * gridDim.y;
+        if (t >= ntiles) break;
+        const int buf = j & 1;
+        const bool w = mbar_wait(smem_addr(&s_bar[buf]), (uint32_t)((j >> 1) & 1));
+        if (!__syncthreads_and(w)) { ok = false; break; }
+        const float *er = Eb + (size_t)(buf * VT_V + vl) * ER;
+        float acc[VT_FPT][3];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
+        // sequential fused multiply-add over k for every output (the order the oracle uses)
+        int k = 0;
+        for (; k + 4 <= K; k += 4) {
+            const float4 ex = *reinterpret_cast<const float4 *>(er + k);
+            const float4 ey = *reinterpret_cast<const float4 *>(er + KP + k);
+            const float4 ez = *reinterpret_cast<const float4 *>(er + 2 * KP + k);
+            const float exv[4] = {ex.x, ex.y, ex.z, ex.w}, eyv[4] = {ey.x, ey.y, ey.z, ey.w};
+            const float ezv[4] = {ez.x, ez.y, ez.z, ez.w};
 #pragma unroll
-            for (int h = 0; h < VT_VPT; ++h) {
-                e[0][j][h] = e0p[(k + j) * VT_PITCH + 32 * h];
-                e[1][j][h] = e1p[(k + j) * VT_PITCH + 32 * h];
-                e[2][j][h] = e2p[(k + j) * VT_PITCH + 32 * h];
-            }
+            for (int q = 0; q < VT_FPT; ++q) {
+                const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
+                const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
-        for (int q = 0; q < VT_FPT; ++q) {
-            const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
-            const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int h = 0; h < VT_VPT; ++h) {
-                    acc[q][h][0] = fmaf(e[0][j][h], xv[j], acc[q][h][0]);
-                    acc[q][h][1] = fmaf(e[1][j][h], xv[j], acc[q][h][1]);
-                    acc[q][h][2] = fmaf(e[2][j][h], xv[j], acc[q][h][2]);
+                for (int jj = 0; jj < 4; ++jj) {
+                    acc[q][0] = fmaf(exv[jj], xv[jj], acc[q][0]);
+                    acc[q][1] = fmaf(eyv[jj], xv[jj], acc[q][1]);
+                    acc[q][2] = fmaf(ezv[jj], xv[jj], acc[q][2]);
                 }
-        }
-    }
-    for (; k < K; ++k) {
-        float e[3][VT_VPT];
-#pragma unroll
-        for (int h = 0; h < VT_VPT; ++h) {
-            e[0][h] = e0p[k * VT_PITCH + 32 * h];
-            e[1][h] = e1p[k * VT_PITCH + 32 * h];
-            e[2][h] = e2p[k * VT_PITCH + 32 * h];
-        }
-#pragma unroll
-        for (int q = 0; q < VT_FPT; ++q) {
-            const float xv = xr[q * KP + k];
-#pragma unroll
-            for (int h = 0; h < VT_VPT; ++h) {
-                acc[q][h][0] = fmaf(e[0][h], xv, acc[q][h][0]);
-                acc[q][h][1] = fmaf(e[1][h], xv, acc[q][h][1]);
-                acc[q][h][2] = fmaf(e[2][h], xv, acc[q][h][2]);
             }
         }
-    }
+        for (; k < K; ++k) {
+            const float ex = er[k], ey = er[KP + k], ez = er[2 * KP + k];
 #pragma unroll
-    for (int h = 0; h < VT_VPT; ++h) {
-        const int v = v0 + vl + 32 * h;
-        if (v >= m.V) continue;
-        const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
-#pragma unroll
-        for (int q = 0; q < VT_FPT; ++q) {
-            const int fl = threadIdx.y * VT_FPT + q;
-            if (!s_render[fl]) continue;
-            const int f = s_frame[fl];
-            const float *R = Fs + fl * VT_FR, *tau = R + 9, *cam = R + 12;
-            const float X0 = mx + acc[q][h][0], Y0 = my + acc[q][h][1], Z0 = mz + acc[q][h][2];
-            const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
-            const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
-            const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
-            float *g = b.geo + (size_t)f * 6 * m.V;
-            g[v] = X0;
-            g[m.V + v] = Y0;
-            g[2 * m.V + v] = Z0;
-            b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
+            for (int q = 0; q < VT_FPT; ++q) {
+                const float xv = xr[q * KP + k];
+                acc[q][0] = fmaf(ex, xv, acc[q][0]);
+                acc[q][1] = fmaf(ey, xv, acc[q][1]);
+                acc[q][2] = fmaf(ez, xv, acc[q][2]);
+            }
         }
+        const int v = t * VT_V + vl;
+        if (v < m.V) {
+            const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
+#pragma unroll
+            for (int q = 0; q < VT_FPT; ++q) {
+                const int fl = threadIdx.y * VT_FPT + q;
+                if (!s_render[fl]) continue;
+                const int f = s_frame[fl];
+                const float *R = Fs + fl * VT_FR, *tau = R + 9, *cam = R + 12;
+                const float X0 = mx + acc[q][0], Y0 = my + acc[q][1], Z0 = mz + acc[q][2];
+                const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
+                const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
+                const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
+                float *g = b.geo + (size_t)f * 6 * m.V;
+                g[v] = X0;
+                g[m.V + v] = Y0;
+                g[2 * m.V + v] = Z0;
+                b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
+            }
+        }
+        __syncthreads();                       // every thread is done with this buffer
+        if (tid == 0) issue(j + 2);
+    }
+    if (!ok) {
+        // copies of tiles j and j + 1 may still be in flight: wait for them (bounded) before
+        // the block's shared memory is released
+        if (tid == 0) {
+            atomicOr(b.err, 2);
+            mbar_wait(smem_addr(&s_bar[j & 1]), (uint32_t)((j >> 1) & 1));
+            if (blockIdx.y + (j + 1) * gridDim.y < ntiles)
+                mbar_wait(smem_addr(&s_bar[(j + 1) & 1]), (uint32_t)(((j + 1) >> 1) & 1));
+        }
+        __syncthreads();
     }
 }
 

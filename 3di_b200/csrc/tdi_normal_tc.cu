@@ -28,7 +28,6 @@ constexpr int TC_MAXN = 128;                      // accumulator columns at most
 constexpr int TC_PIECE = TC_M * TC_KS * 2;        // bytes of one BF16 piece of a stage (16 KB)
 constexpr int TC_SMEM = 3 * TC_PIECE;             // dynamic shared memory: hi, mid, lo pieces
 constexpr int TC_TMEM_COLS = 128;                 // the accumulator
-constexpr long long TC_WAIT_CYCLES = 2000000000ll;
 constexpr int TC_BPF = 32;                        // blocks per frame (each loops over chunks)
 static_assert(TC_THREADS == NE_CH, "one thread per fragment of a chunk");
 
@@ -42,11 +41,6 @@ __host__ __device__ __forceinline__ int tc_pitch(int KT) { return (KT + 1 + 3) &
 __host__ __device__ __forceinline__ size_t tc_part_bytes(int KT)
 {
     return (size_t)tc_pitch(KT) * tc_pitch(KT) * sizeof(float);
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
 }
 
 // Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8 rows x 16 bytes;
@@ -74,25 +68,6 @@ __device__ __forceinline__ void umma_commit(uint32_t bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
-}
-
-// Waits for the completion of the phase with the given parity; false after ~1 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    const long long t0 = clock64();
-    for (;;) {
-        uint32_t done;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
-        if (done) return true;
-        if (clock64() - t0 > TC_WAIT_CYCLES) return false;
-    }
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
