@@ -398,12 +398,14 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
     d.V = V; d.T = T; d.K = K; d.KP = round4(K); d.KT = K + 6; d.KTP = round4(K + 6);
     float *mean, *E, *tex, *epsb;
     int32_t *tl, *lis, *order, *tlo;
+    int4 *tl4, *tlo4;
     auto cleanup = [&](tdi_status st) { for (void *p : m->allocs) cudaFree(p); delete m; return st; };
     tdi_status st;
     if ((st = dalloc(m->allocs, &mean, 3 * (size_t)V)) || (st = dalloc(m->allocs, &E, (size_t)V * 3 * d.KP)) ||
         (st = dalloc(m->allocs, &tex, (size_t)V)) || (st = dalloc(m->allocs, &tl, 3 * (size_t)T)) ||
         (st = dalloc(m->allocs, &lis, (size_t)NL)) || (st = dalloc(m->allocs, &epsb, 4 * (size_t)K)) ||
-        (st = dalloc(m->allocs, &order, (size_t)T)) || (st = dalloc(m->allocs, &tlo, 3 * (size_t)T)))
+        (st = dalloc(m->allocs, &order, (size_t)T)) || (st = dalloc(m->allocs, &tlo, 3 * (size_t)T)) ||
+        (st = dalloc(m->allocs, &tl4, (size_t)T)) || (st = dalloc(m->allocs, &tlo4, (size_t)T)))
         return cleanup(st);
     // Internal vertex numbering: vertices are stored in Morton order of their mean-shape (x, y)
     // position (slot), so that the corners of neighbouring triangles sit in neighbouring
@@ -455,6 +457,9 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
     for (int r = 0; r < 3; ++r)
         for (int s = 0; s < T; ++s) tlo_h[(size_t)r * T + s] = tls[(size_t)r * T + tord[s]];
     for (int i = 0; i < NL; ++i) lis_h[i] = m->vslot[desc->landmarks[i]];
+    std::vector<int4> tl4_h(T), tlo4_h(T);
+    for (int t = 0; t < T; ++t) tl4_h[t] = make_int4(tls[t], tls[(size_t)T + t], tls[2 * (size_t)T + t], 0);
+    for (int s2 = 0; s2 < T; ++s2) tlo4_h[s2] = make_int4(tlo_h[s2], tlo_h[(size_t)T + s2], tlo_h[2 * (size_t)T + s2], tord[s2]);
     std::vector<float> mean_h(3 * (size_t)V), tex_h(V);
     for (int c = 0; c < 3; ++c)
         for (int s = 0; s < V; ++s) mean_h[(size_t)c * V + s] = desc->mean[(size_t)c * V + vord[s]];
@@ -475,9 +480,11 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
         cudaMemcpy(lis, lis_h.data(), sizeof(int32_t) * NL, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(epsb, eb.data(), sizeof(float) * eb.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(order, tord.data(), sizeof(int32_t) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(tlo, tlo_h.data(), sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(tlo, tlo_h.data(), sizeof(int32_t) * 3 * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tl4, tl4_h.data(), sizeof(int4) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(tlo4, tlo4_h.data(), sizeof(int4) * T, cudaMemcpyHostToDevice) != cudaSuccess)
         return cleanup(fail(TDI_ERR_CUDA, "model upload failed"));
-    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb; d.tri_order = order; d.tlo = tlo;
+    d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb; d.tri_order = order; d.tlo = tlo; d.tl4 = tl4; d.tlo4 = tlo4;
     *out = m;
     return TDI_OK;
 }
@@ -515,7 +522,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
-    A(d.ctl, F); A(d.act, F); A(d.geo, F * 6 * md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
+    A(d.ctl, F); A(d.act, F); A(d.geo, F * (size_t)md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
     A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8)); A(d.err, 1); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 2);
     A(d.prof_frames, 1);
@@ -743,15 +750,15 @@ tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, 
     case 6: {
         if (capacity < (int64_t)(6 * (size_t)m.V * sizeof(float))) return fail(TDI_ERR_INVALID, "destination too small");
         // stored by slot; returned in the caller's vertex numbering
-        std::vector<float> g(3 * (size_t)m.V);
+        std::vector<float4> g(m.V);
         std::vector<float4> pj(m.V);
-        TDI_CUDA(cudaMemcpy(g.data(), d.geo + (size_t)frame * 6 * m.V, 3 * (size_t)m.V * sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(g.data(), d.geo + (size_t)frame * m.V, (size_t)m.V * sizeof(float4), cudaMemcpyDeviceToHost));
         TDI_CUDA(cudaMemcpy(pj.data(), d.proj + (size_t)frame * m.V, (size_t)m.V * sizeof(float4), cudaMemcpyDeviceToHost));
         float *o = static_cast<float *>(dst);
         const std::vector<int32_t> &vs = b->m->vslot;
         for (int v = 0; v < m.V; ++v) {
             const size_t sl = (size_t)vs[v];
-            o[v] = g[sl]; o[m.V + v] = g[m.V + sl]; o[2 * (size_t)m.V + v] = g[2 * (size_t)m.V + sl];
+            o[v] = g[sl].x; o[m.V + v] = g[sl].y; o[2 * (size_t)m.V + v] = g[sl].z;
             o[3 * (size_t)m.V + v] = pj[sl].x; o[4 * (size_t)m.V + v] = pj[sl].y; o[5 * (size_t)m.V + v] = pj[sl].z;
         }
         n = 6 * (int64_t)m.V;

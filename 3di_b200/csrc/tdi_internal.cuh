@@ -91,6 +91,8 @@ struct DModel {
     const float *eps_b;      // [4][K]: lb, ub, lb_ft, ub_ft
     const int32_t *tri_order;// [T] triangles in Morton order of their mean-shape centroids
     const int32_t *tlo;      // [3][T] corner slots of the triangles in tri_order
+    const int4 *tl4;         // [T] corner slots (b, c, a, 0): one 16-byte gather per triangle
+    const int4 *tlo4;        // [T] in tri_order: corner slots and the triangle id (b, c, a, tri)
 };
 
 // Device view of a batch of frames and its working set.
@@ -114,7 +116,7 @@ struct DBatch {
     int32_t *act;            // [F] frames running the stage at the start of the round, ascending
     int32_t nact;            // entries of act
     // per-render working set
-    float *geo;              // [F][6][V]: X0, Y0, Z0 planes (planes 3-5 unused)
+    float4 *geo;             // [F][V]: X0, Y0, Z0 and the albedo of the vertex (slot order)
     float4 *proj;            // [F][V]: xp, yp, camera Z, 0 -- what the raster gathers
     unsigned long long *zbuf;// [F][NPIX]
     uint32_t *tri_mask;      // [F][ceil(T/32)] triangles with fragments in the raster in flight

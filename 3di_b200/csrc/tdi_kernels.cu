@@ -173,8 +173,8 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 // strided set of 32-vertex tiles; each tile's basis rows (32 x 3 x KP floats, contiguous in
 // HBM) are brought into shared memory by the TMA engine, one bulk copy per vertex row,
 // double-buffered so that the next tile streams in while this one is computed. A thread
-// owns one vertex x 8 frames (24 FMA chains). geo[f] = [X0 | Y0 | Z0] planes of V floats
-// (vertex slots); proj[f][slot] = (xp, yp, camera Z, 0).
+// owns one vertex x 8 frames (24 FMA chains). geo[f][slot] = (X0, Y0, Z0, albedo);
+// proj[f][slot] = (xp, yp, camera Z, 0).
 
 constexpr int VT_V = 32;                                   // vertices per tile (one per lane)
 constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
         }
         const int v = t * VT_V + vl;
         if (v < m.V) {
-            const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v];
+            const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v], tx = m.tex[v];
 #pragma unroll
             for (int q = 0; q < VT_FPT; ++q) {
                 const int fl = threadIdx.y * VT_FPT + q;
@@ -303,10 +303,7 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
                 const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
                 const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
                 const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
-                float *g = b.geo + (size_t)f * 6 * m.V;
-                g[v] = X0;
-                g[m.V + v] = Y0;
-                g[2 * m.V + v] = Z0;
+                b.geo[(size_t)f * m.V + v] = make_float4(X0, Y0, Z0, tx);
                 b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
             }
         }
@@ -337,13 +334,14 @@ __device__ __forceinline__ void landmark_G(const DModel &m, const DBatch &b, int
                                            const float *R, int i, float G[4])
 {
     const float *tau = x + m.K;
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float4 *geo = b.geo + (size_t)f * m.V;
     const float *cam = b.cam + f * 4;
     const float fs = b.face_size[f];
     const float *bnd = b.bounds + (size_t)f * 4 * NL;
     const float xl = b.xl[f * NL + i], yl = b.yl[f * NL + i];
     const int v = m.lis[i];
-    const float p0 = geo[v], p1 = geo[m.V + v], p2 = geo[2 * m.V + v];
+    const float4 pv = geo[v];
+    const float p0 = pv.x, p1 = pv.y, p2 = pv.z;
     const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
     const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
     const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
@@ -553,10 +551,11 @@ __global__ void __launch_bounds__(RD_THREADS) k_raster_depth(DModel m, DBatch b)
     const int s_begin = blockIdx.x * per_block, s_end = min(T, s_begin + per_block);
     uint32_t flags = 0;
     for (int s = s_begin + (int)threadIdx.x; s < s_end; s += RD_THREADS) {
-        const int idx = __ldg(m.tri_order + s);
-        const float4 pb = __ldg(pj + __ldg(m.tlo + s));
-        const float4 pc = __ldg(pj + __ldg(m.tlo + T + s));
-        const float4 pa = __ldg(pj + __ldg(m.tlo + 2 * T + s));
+        const int4 tq = __ldg(m.tlo4 + s);
+        const int idx = tq.w;
+        const float4 pb = __ldg(pj + tq.x);
+        const float4 pc = __ldg(pj + tq.y);
+        const float4 pa = __ldg(pj + tq.z);
         const unsigned long long key = zkey(tag, pb.z, idx);
         const int nf = tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, flags,
                                    [&](int, uint32_t px, float, float) { atomicMin(zb + px, key); });
@@ -657,9 +656,10 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
         bool sv[NTMP] = {false, false, false, false};
         if (e < e_end) {
             const int idx = __ldcg(list + e);
-            const float4 pb = __ldg(pj + __ldg(m.tl + idx));
-            const float4 pc = __ldg(pj + __ldg(m.tl + T + idx));
-            const float4 pa = __ldg(pj + __ldg(m.tl + 2 * T + idx));
+            const int4 tc = __ldg(m.tl4 + idx);
+            const float4 pb = __ldg(pj + tc.x);
+            const float4 pc = __ldg(pj + tc.y);
+            const float4 pa = __ldg(pj + tc.z);
             const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
             uint32_t fl2 = 0;
             tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, fl2, [&](int r, uint32_t px, float, float) {
@@ -717,9 +717,10 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
         int idx = -1;
         if (e < e_end) {
             idx = __ldcg(list + e);
-            const float4 pb = __ldg(pj + __ldg(m.tl + idx));
-            const float4 pc = __ldg(pj + __ldg(m.tl + T + idx));
-            const float4 pa = __ldg(pj + __ldg(m.tl + 2 * T + idx));
+            const int4 tc = __ldg(m.tl4 + idx);
+            const float4 pb = __ldg(pj + tc.x);
+            const float4 pc = __ldg(pj + tc.y);
+            const float4 pa = __ldg(pj + tc.z);
             const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
             const unsigned long long mykey = zkey(tag, pb.z, idx);
             uint32_t fl2 = 0;
@@ -792,16 +793,16 @@ __device__ __forceinline__ void camera_coords(const float *R, const float *tau, 
     Z = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
 }
 
-__device__ __forceinline__ Shading shade(const DModel &m, const float *geo, const Fragment &fr,
+__device__ __forceinline__ Shading shade(const DModel &m, const float4 *geo, const Fragment &fr,
                                          const float *R, const float *tau, const float *lam,
                                          float Lint)
 {
-    const int V = m.V, T = m.T, tri = fr.tri;
-    const int ib = m.tl[tri], ic = m.tl[T + tri], ia = m.tl[2 * T + tri];
+    const int4 tc = __ldg(m.tl4 + fr.tri);
     const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
-    const float b0x = geo[ib], b0y = geo[V + ib], b0z = geo[2 * V + ib];
-    const float c0x = geo[ic], c0y = geo[V + ic], c0z = geo[2 * V + ic];
-    const float a0x = geo[ia], a0y = geo[V + ia], a0z = geo[2 * V + ia];
+    const float4 gb = geo[tc.x], gc = geo[tc.y], ga4 = geo[tc.z];
+    const float b0x = gb.x, b0y = gb.y, b0z = gb.z;
+    const float c0x = gc.x, c0y = gc.y, c0z = gc.z;
+    const float a0x = ga4.x, a0y = ga4.y, a0z = ga4.z;
     const float n_vx = b0x - a0x, n_vy = b0y - a0y, n_vz = b0z - a0z;
     const float n_wx = c0x - a0x, n_wy = c0y - a0y, n_wz = c0z - a0z;
     const float nrx = n_vy * n_wz - n_vz * n_wy;
@@ -818,7 +819,7 @@ __device__ __forceinline__ Shading shade(const DModel &m, const float *geo, cons
                 + s.nn[1] * ((R[3] * d0 + R[4] * d1) + R[5] * d2))
                + s.nn[2] * ((R[6] * d0 + R[7] * d1) + R[8] * d2);
     Id = Id - ((s.nn[0] * s.p[0] + s.nn[1] * s.p[1]) + s.nn[2] * s.p[2]);
-    const float t = (m.tex[ib] * al + m.tex[ic] * be) + m.tex[ia] * ga;
+    const float t = (gb.w * al + gc.w * be) + ga4.w * ga;
     s.tex = t + (Lint * t) * Id;
     s.Id = Id;
     float bX, bY, bZ, cX, cY, cZ, aX, aY, aZ;
@@ -863,8 +864,9 @@ __device__ __forceinline__ void target_grad(const float *im, int ks, float &gxn,
     gyn = (2.0f * bb) / hh;
 }
 
-constexpr int RENDER_THREADS = 512;
-constexpr int RENDER_SMEM_FLOATS = 50 * 1024;   // two region buffers of up to 25,600 floats
+constexpr int RENDER_THREADS = 256;
+constexpr int RENDER_SMEM_FLOATS = 16 * 1024;   // two region buffers of up to 8,192 pixels
+constexpr int RENDER_UNROLL = 4;                 // fragments whose gathers are in flight together
 
 __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, Cfg c, int stage)
 {
@@ -874,57 +876,70 @@ __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, C
     if (threadIdx.x == 0) prof_count(b, KID_RENDER);
     extern __shared__ float rsm[];
     __shared__ double s_red[RENDER_THREADS / 32];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = RENDER_THREADS / 32;
     const int N = ctl.N;
     const bool border = ctl.bbox[0] < 1 || ctl.bbox[1] > DIM - 2 || ctl.bbox[2] < 1 || ctl.bbox[3] > DIM - 2;
     const int rx0 = border ? 0 : max(0, ctl.bbox[0] - 8), rx1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[1] + 8);
     const int ry0 = border ? 0 : max(0, ctl.bbox[2] - 8), ry1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[3] + 8);
     const int rw = rx1 - rx0 + 1, rh = ry1 - ry0 + 1;
     const int area = rw * rh;
+    // the region (fragment box + 8 px) in shared memory, or in the frame's global buffer when
+    // it is larger than 8,192 pixels
     float *A, *B;
     if (2 * area <= RENDER_SMEM_FLOATS) { A = rsm; B = rsm + area; }
     else { A = b.img + (size_t)f * 2 * NPIX; B = A + NPIX; }
     for (int i = tid; i < area; i += RENDER_THREADS) A[i] = 0.0f;
     __syncthreads();
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float4 *geo = b.geo + (size_t)f * m.V;
     const float *R = b.R + f * 9;
     const float *xsrc = stage == ST_LAMBDA ? b.x : b.xe;
     const float *tau = xsrc + (size_t)f * m.KTP + m.K;
     const float *lam = (stage == ST_LAMBDA && ctl.mode == M_TRIAL) ? b.lam_ls + f * 4 : b.lam + f * 4;
     const float Lint = b.Lint[f];
     const Fragment *frags = b.frag + (size_t)f * NMAX;
-    for (int n = tid; n < N; n += RENDER_THREADS) {
-        const Fragment fr = frags[n];
-        if (fr.pix_owner & 0x80000000u) {
-            const Shading s = shade(m, geo, fr, R, tau, lam, Lint);
-            const int p = fr.pix_owner & 0xFFFF;
-            A[((p >> 8) - rx0) * rh + ((p & 255) - ry0)] = s.tex;
+    for (int n0 = tid; n0 < N; n0 += RENDER_THREADS * RENDER_UNROLL) {
+        Fragment fr[RENDER_UNROLL];
+#pragma unroll
+        for (int u = 0; u < RENDER_UNROLL; ++u) {
+            const int n = n0 + u * RENDER_THREADS;
+            fr[u] = n < N ? frags[n] : Fragment{0u, 0, 0.0f, 0.0f};
+        }
+#pragma unroll
+        for (int u = 0; u < RENDER_UNROLL; ++u) {
+            if (fr[u].pix_owner & 0x80000000u) {
+                const Shading sh = shade(m, geo, fr[u], R, tau, lam, Lint);
+                const int p = fr[u].pix_owner & 0xFFFF;
+                A[((p >> 8) - rx0) * rh + ((p & 255) - ry0)] = sh.tex;
+            }
         }
     }
     __syncthreads();
-    // rows: along the contiguous (y) index
-    for (int i = tid; i < area; i += RENDER_THREADS) {
-        const int xl = i / rh, yl = i - xl * rh;
-        float s = 0.0f;
-        for (int j = -KRAD; j <= KRAD; ++j) {
-            const int yy = yl + j;
-            const float v = (yy >= 0 && yy < rh) ? A[xl * rh + yy] : 0.0f;
-            s = s + c.taps[KRAD - j] * v;
+    // rows: along the contiguous (y) index; warps take columns, lanes take rows
+    for (int xl = warp; xl < rw; xl += NW)
+        for (int yl = lane; yl < rh; yl += 32) {
+            float s = 0.0f;
+#pragma unroll
+            for (int j = -KRAD; j <= KRAD; ++j) {
+                const int yy = yl + j;
+                const float v = (yy >= 0 && yy < rh) ? A[xl * rh + yy] : 0.0f;
+                s = s + c.taps[KRAD - j] * v;
+            }
+            B[xl * rh + yl] = s;
         }
-        B[i] = s;
-    }
     __syncthreads();
     // columns: along the strided (x) index
-    for (int i = tid; i < area; i += RENDER_THREADS) {
-        const int xl = i / rh, yl = i - xl * rh;
-        float s = 0.0f;
-        for (int j = -KRAD; j <= KRAD; ++j) {
-            const int xx = xl + j;
-            const float v = (xx >= 0 && xx < rw) ? B[xx * rh + yl] : 0.0f;
-            s = s + c.taps[KRAD - j] * v;
+    for (int xl = warp; xl < rw; xl += NW)
+        for (int yl = lane; yl < rh; yl += 32) {
+            float s = 0.0f;
+#pragma unroll
+            for (int j = -KRAD; j <= KRAD; ++j) {
+                const int xx = xl + j;
+                const float v = (xx >= 0 && xx < rw) ? B[xx * rh + yl] : 0.0f;
+                s = s + c.taps[KRAD - j] * v;
+            }
+            A[xl * rh + yl] = s;
         }
-        A[i] = s;
-    }
     __syncthreads();
     const float *tgt = b.target + (size_t)f * NPIX;
     float *fg = b.fgrad + (size_t)f * 5 * NMAX;
@@ -940,11 +955,11 @@ __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, C
         corr += (double)gxn * (double)sxn + (double)gyn * (double)syn;
     }
     for (int o = 16; o > 0; o >>= 1) corr += __shfl_down_sync(0xffffffffu, corr, o);
-    if ((tid & 31) == 0) s_red[tid >> 5] = corr;
+    if (lane == 0) s_red[warp] = corr;
     __syncthreads();
     if (tid == 0) {
         double s = 0.0;
-        for (int w = 0; w < RENDER_THREADS / 32; ++w) s += s_red[w];
+        for (int w = 0; w < NW; ++w) s += s_red[w];
         ctl.corr = s;
     }
 }
@@ -1169,9 +1184,9 @@ __global__ void __launch_bounds__(JAC_WARPS * 32) k_jacobian(DModel m, DBatch b)
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_JACOBIAN);
-    const int N = ctl.N, K = m.K, KP = m.KP, T = m.T, V = m.V;
+    const int N = ctl.N, K = m.K, KP = m.KP, V = m.V;
     const int lane = threadIdx.x & 31;
-    const float *geo = b.geo + (size_t)f * 6 * V;
+    const float4 *geo = b.geo + (size_t)f * V;
     const float *R = b.R + f * 9, *dR = b.dR + f * 27;
     const float *tau = b.xe + (size_t)f * m.KTP + K;
     const float phix = b.cam[f * 4], phiy = b.cam[f * 4 + 1];
@@ -1181,11 +1196,13 @@ __global__ void __launch_bounds__(JAC_WARPS * 32) k_jacobian(DModel m, DBatch b)
     for (int n = blockIdx.x * JAC_WARPS + (threadIdx.x >> 5); n < N; n += wstride) {
         const Fragment fr = frags[n];
         const int tri = fr.tri;
-        const int ib = m.tl[tri], ic = m.tl[T + tri], ia = m.tl[2 * T + tri];
+        const int4 tc = __ldg(m.tl4 + tri);
+        const int ib = tc.x, ic = tc.y, ia = tc.z;
         const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
-        const float b0x = geo[ib], b0y = geo[V + ib], b0z = geo[2 * V + ib];
-        const float c0x = geo[ic], c0y = geo[V + ic], c0z = geo[2 * V + ic];
-        const float a0x = geo[ia], a0y = geo[V + ia], a0z = geo[2 * V + ia];
+        const float4 gb = geo[ib], gc = geo[ic], ga4 = geo[ia];
+        const float b0x = gb.x, b0y = gb.y, b0z = gb.z;
+        const float c0x = gc.x, c0y = gc.y, c0z = gc.z;
+        const float a0x = ga4.x, a0y = ga4.y, a0z = ga4.z;
         const float px = (b0x * al + c0x * be) + a0x * ga;
         const float py = (b0y * al + c0y * be) + a0y * ga;
         const float pz = (b0z * al + c0z * be) + a0z * ga;
@@ -1494,7 +1511,7 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     const float *x = b.x + (size_t)f * KTP;       // the accepted point (= evaluation point)
     const float *R = b.R + f * 9, *dR = b.dR + f * 27;
     const float *tau = x + K;
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float4 *geo = b.geo + (size_t)f * m.V;
     const float *cam = b.cam + f * 4;
     const float phix = cam[0], phiy = cam[1], cx = cam[2], cy = cam[3];
     const float fs = b.face_size[f];
@@ -1502,7 +1519,8 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     const float *xl = b.xl + f * NL, *yl = b.yl + f * NL;
     if (tid < NL) {
         const int v = m.lis[tid];
-        const float p0 = geo[v], p1 = geo[m.V + v], p2 = geo[2 * m.V + v];
+        const float4 pv = geo[v];
+        const float p0 = pv.x, p1 = pv.y, p2 = pv.z;
         s_p[tid][0] = p0; s_p[tid][1] = p1; s_p[tid][2] = p2;
         const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
         const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
@@ -1691,7 +1709,7 @@ __global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
     __shared__ double s_L[9], s_y[3];
     __shared__ float s_g[3];
     const int tid = threadIdx.x, N = ctl.N;
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float4 *geo = b.geo + (size_t)f * m.V;
     const float *R = b.R + f * 9;
     const float *tau = b.x + (size_t)f * m.KTP + m.K;
     const float *lam = b.lam + f * 4;
@@ -1703,7 +1721,8 @@ __global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
         const Fragment fr = frags[n];
         const int tri = fr.tri;
         const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
-        const float t = (m.tex[m.tl[tri]] * al + m.tex[m.tl[m.T + tri]] * be) + m.tex[m.tl[2 * m.T + tri]] * ga;
+        const int4 tc = __ldg(m.tl4 + tri);
+        const float t = (geo[tc.x].w * al + geo[tc.y].w * be) + geo[tc.z].w * ga;
         const float Lt = Lint * t;
         const float r0 = Lt * s.nn[0], r1 = Lt * s.nn[1], r2 = Lt * s.nn[2];
         for (int j = 0; j < 3; ++j) Jl[(size_t)n * 4 + j] = (r0 * R[j] + r1 * R[j + 3]) + r2 * R[j + 6];
@@ -1790,7 +1809,7 @@ __global__ void k_paint(DModel m, DBatch b, float *images, int32_t *tri_map)
     __syncthreads();
     // the clear above and the writes below touch disjoint work of one frame only when the
     // grid has a single block in x; the host launches it that way
-    const float *geo = b.geo + (size_t)f * 6 * m.V;
+    const float4 *geo = b.geo + (size_t)f * m.V;
     const float *R = b.R + f * 9;
     const float *tau = b.xe + (size_t)f * m.KTP + m.K;
     const float *lam = b.lam + f * 4;
