@@ -316,7 +316,7 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
     }
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
-    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(128), L.smem_solve(), L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(256), L.smem_solve(), L.s, L.m, L.b, c, stage));
     return TDI_OK;
 }
 

@@ -1618,46 +1618,51 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
 // first trial of the line search. Column j: diagonal by one thread, then the rows below in
 // parallel, each a sequential dot product over k (the oracle's order).
 
+// FP64 Cholesky factor and solve of one frame's system by the whole block (solver.h:70-105
+// with cuSOLVER DPOTRF/DPOTRS in the reference). L is column-major [n][n], holding H on entry.
+// Right-looking: after column j is scaled, every trailing entry is updated at once; each
+// entry receives its updates in increasing j, i.e. the same sequence of subtractions as the
+// left-looking dot products of the oracle. Forward substitution by columns (terms in
+// increasing k), back substitution by columns (terms in decreasing k, the oracle's order).
+// Every thread recomputes the pivot it needs, so a step costs one or two barriers.
 __device__ int chol_solve_block(double *L, int n, const float *g, double *y)
 {
-    __shared__ int s_ok;
-    const int tid = threadIdx.x;
-    if (tid == 0) s_ok = 1;
-    __syncthreads();
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, nw = nt >> 5;
     for (int j = 0; j < n; ++j) {
-        if (tid == 0) {
-            double s = L[j * n + j];
-            for (int k = 0; k < j; ++k) s -= L[k * n + j] * L[k * n + j];
-            if (!(s > 0.0)) s_ok = 0;
-            L[j * n + j] = sqrt(s);
-        }
+        const double s = L[j * n + j];
+        if (!(s > 0.0)) return 0;               // every thread sees the same pivot
+        const double ljj = sqrt(s);
+        for (int i = j + 1 + tid; i < n; i += nt) L[j * n + i] = L[j * n + i] / ljj;
         __syncthreads();
-        if (!s_ok) break;
-        const double ljj = L[j * n + j];
-        for (int i = j + 1 + tid; i < n; i += blockDim.x) {
-            double t = L[j * n + i];
-            for (int k = 0; k < j; ++k) t -= L[k * n + i] * L[k * n + j];
-            L[j * n + i] = t / ljj;
+        if (tid == 0) L[j * n + j] = ljj;
+        // trailing update of the lower triangle, entries (i, l) with j < l <= i < n: warps
+        // take columns l, lanes take rows i
+        for (int l = j + 1 + (tid >> 5); l < n; l += nw) {
+            const double llj = L[j * n + l];
+            for (int i = l + lane; i < n; i += 32) L[l * n + i] -= L[j * n + i] * llj;
         }
         __syncthreads();
     }
-    if (tid == 0 && s_ok) {
-        for (int i = 0; i < n; ++i) {
-            double t = (double)g[i];
-            for (int k = 0; k < i; ++k) t -= L[k * n + i] * y[k];
-            y[i] = t / L[i * n + i];
-        }
-        for (int i = n - 1; i >= 0; --i) {
-            double t = y[i];
-            for (int k = i + 1; k < n; ++k) t -= L[i * n + k] * y[k];
-            y[i] = t / L[i * n + i];
-        }
+    for (int i = tid; i < n; i += nt) y[i] = (double)g[i];
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const double yk = y[k] / L[k * n + k];
+        for (int i = k + 1 + tid; i < n; i += nt) y[i] -= L[k * n + i] * yk;
+        __syncthreads();
+        if (tid == 0) y[k] = yk;
     }
     __syncthreads();
-    return s_ok;
+    for (int k = n - 1; k >= 0; --k) {
+        const double yk = y[k] / L[k * n + k];
+        for (int i = tid; i < k; i += nt) y[i] -= L[i * n + k] * yk;
+        __syncthreads();
+        if (tid == 0) y[k] = yk;
+    }
+    __syncthreads();
+    return 1;
 }
 
-__global__ void __launch_bounds__(128) k_solve(DModel m, DBatch b, Cfg c, int stage)
+__global__ void __launch_bounds__(256) k_solve(DModel m, DBatch b, Cfg c, int stage)
 {
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
@@ -1668,10 +1673,8 @@ __global__ void __launch_bounds__(128) k_solve(DModel m, DBatch b, Cfg c, int st
     double *L = ssm;             // [KT][KT]
     double *y = L + KT * KT;     // [KT]
     const float *H = b.H + (size_t)f * KTP * KTP;
-    for (int i = threadIdx.x; i < KT * KT; i += blockDim.x) {
-        const int col = i / KT, row = i - col * KT;
-        L[i] = (double)H[(size_t)col * KTP + row];
-    }
+    for (int col = threadIdx.x >> 5; col < KT; col += blockDim.x >> 5)
+        for (int row = threadIdx.x & 31; row < KT; row += 32) L[col * KT + row] = (double)H[(size_t)col * KTP + row];
     __syncthreads();
     const float *gv = b.g + (size_t)f * KTP;
     const int ok = chol_solve_block(L, KT, gv, y);

@@ -671,9 +671,12 @@ static int solve(const real *H, const real *g, int n, real *d)
             for (int k = 0; k < i; ++k) t -= L[k * n + i] * y[k];
             y[i] = t / L[i * n + i];
         }
+        /* back substitution: the terms of row i are subtracted in decreasing k (the order in
+         * which the y_k become known; cuSOLVER's DPOTRS order in the reference is the
+         * library's) */
         for (int i = n - 1; i >= 0; --i) {
             double t = y[i];
-            for (int k = i + 1; k < n; ++k) t -= L[i * n + k] * y[k];
+            for (int k = n - 1; k > i; --k) t -= L[i * n + k] * y[k];
             y[i] = t / L[i * n + i];
         }
         for (int i = 0; i < n; ++i) d[i] = (real)(-y[i]);
