@@ -1279,20 +1279,25 @@ constexpr int NE_BPF = 32;                   // blocks per frame
 constexpr int NE_MAXCH = NMAX / NE_CH;       // chunk partials per frame at most
 static_assert(NE_THREADS == NE_CH && NE_SUB == 32 && NE_THREADS == 8 * 32, "thread mapping of the row build");
 
-// Upper-triangle 4x4 block (bi <= bj) owned by thread t, or -1.
-__device__ __forceinline__ void ne_block(int t, int nb4, int &bi, int &bj)
+// Accumulator tiles of 4 rows x 8 columns covering the upper triangle (a <= c) of a KTP x KTP
+// matrix with KTP <= 88: row block r4 (rows 4*r4..4*r4+3) needs column blocks c8 >=
+// max(0, ceil((4*r4 - 7) / 8)). NE_TILES threads own one tile each.
+constexpr int NE_TILES = 132;                // tiles for KTP = 88 (22 row blocks x up to 11 column blocks)
+
+__device__ __forceinline__ void ne_tile(int t, int &r4, int &c8)
 {
-    bi = bj = -1;
-    for (int i = 0; i < nb4 && bi < 0; ++i) {
-        const int len = nb4 - i;
-        if (t < len) { bi = i; bj = i + t; } else t -= len;
+    r4 = c8 = -1;
+    for (int r = 0; r < 22; ++r) {
+        const int c0 = max(0, (4 * r - 7 + 7) / 8);
+        const int len = 11 - c0;
+        if (t < len) { r4 = r; c8 = c0 + t; return; }
+        t -= len;
     }
 }
 
 __host__ __device__ __forceinline__ int ne_part_stride(int KTP)
 {
-    const int nb4 = KTP / 4;
-    return nb4 * (nb4 + 1) / 2 * 16 + KTP;
+    return NE_TILES * 32 + KTP;
 }
 
 // Rows of one chunk of NE_CH fragments: per-fragment scalars and neighbour indices are
@@ -1361,14 +1366,17 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
-    extern __shared__ __align__(16) double nesm[];
+    extern __shared__ __align__(16) float nesf[];   // rows [2][2*NE_SUB][KTP], FP32
     const int KTP = m.KTP, KT = m.KT;
     __shared__ ChunkHead hd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int a_low = lane & 7, q_me = 4 * warp + (lane >> 3);
-    const int nb4 = KTP / 4;
-    int bi, bj;
-    ne_block(tid, nb4, bi, bj);
+    // threads below NE_TILES own a 4 x 8 tile of the sum; the next KTP threads own one entry
+    // of the weighted sum; both work on the stage the build has just finished
+    int r4, c8;
+    ne_tile(tid, r4, c8);
+    const int gcol = tid - NE_TILES;
+    const bool gthread = gcol >= 0 && gcol < KTP;
     const int N = ctl.N;
     const int nch = (N + NE_CH - 1) / NE_CH;
     const float *Jf = b.J + (size_t)f * NMAX * KTP;
@@ -1376,24 +1384,23 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
     const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
     const int stride = ne_part_stride(KTP);
     for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        double acc[4][4];
+        double acc[4][8];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
         double gacc = 0.0;
         const int c0 = ch * NE_CH, cnt = min(N, c0 + NE_CH) - c0;
         const int nsub = (cnt + NE_SUB - 1) / NE_SUB;
-        __syncthreads();                          // the previous chunk is done with hd
+        __syncthreads();                          // the previous chunk is done with hd and the rows
         chunk_head(hd, fg, nb, c0, cnt);
         __syncthreads();
-        float v[NE_GRP][4];
-        chunk_prefetch<NE_GRP>(v, hd, Jf, KT, KTP, q_me, cnt, a_low);
         for (int it = 0; it < nsub; ++it) {
-            // rows of stage it (double buffered: the other buffer is being summed)
-            double *rows = nesm + (size_t)(it & 1) * 2 * NE_SUB * KTP;      // [2*NE_SUB][KTP]
+            float *rows = nesf + (size_t)(it & 1) * 2 * NE_SUB * KTP;
             {
+                float v[NE_GRP][4];
                 const int ql = q_me, q = it * NE_SUB + ql;
+                chunk_prefetch<NE_GRP>(v, hd, Jf, KT, KTP, q, cnt, a_low);
                 const float pre = hd.pre[q], diffx = hd.dx[q], diffy = hd.dy[q];
                 const bool live = q < cnt;
 #pragma unroll
@@ -1402,49 +1409,46 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
                     if (a >= KTP) continue;
                     float ox = 0.0f, oy = 0.0f;
                     if (live && a < KT) chain_value(v[g], pre, diffx, diffy, ox, oy);
-                    rows[(2 * ql) * KTP + a] = (double)ox;
-                    rows[(2 * ql + 1) * KTP + a] = (double)oy;
+                    rows[(2 * ql) * KTP + a] = ox;
+                    rows[(2 * ql + 1) * KTP + a] = oy;
                 }
             }
             __syncthreads();
-            if (it + 1 < nsub) chunk_prefetch<NE_GRP>(v, hd, Jf, KT, KTP, (it + 1) * NE_SUB + q_me, cnt, a_low);
             const int cn = min(NE_SUB, cnt - it * NE_SUB);
-            if (bi >= 0) {
+            if (r4 >= 0) {
                 for (int q = 0; q < cn; ++q) {
-                    const double *rx = rows + (2 * q) * KTP, *ry = rx + KTP;
-                    const double2 ax0 = *reinterpret_cast<const double2 *>(rx + 4 * bi);
-                    const double2 ax1 = *reinterpret_cast<const double2 *>(rx + 4 * bi + 2);
-                    const double2 cx0 = *reinterpret_cast<const double2 *>(rx + 4 * bj);
-                    const double2 cx1 = *reinterpret_cast<const double2 *>(rx + 4 * bj + 2);
-                    const double2 ay0 = *reinterpret_cast<const double2 *>(ry + 4 * bi);
-                    const double2 ay1 = *reinterpret_cast<const double2 *>(ry + 4 * bi + 2);
-                    const double2 cy0 = *reinterpret_cast<const double2 *>(ry + 4 * bj);
-                    const double2 cy1 = *reinterpret_cast<const double2 *>(ry + 4 * bj + 2);
-                    const double axv[4] = {ax0.x, ax0.y, ax1.x, ax1.y}, cxv[4] = {cx0.x, cx0.y, cx1.x, cx1.y};
-                    const double ayv[4] = {ay0.x, ay0.y, ay1.x, ay1.y}, cyv[4] = {cy0.x, cy0.y, cy1.x, cy1.y};
+                    const float *rx = rows + (2 * q) * KTP, *ry = rx + KTP;
+                    const float4 ax4 = *reinterpret_cast<const float4 *>(rx + 4 * r4);
+                    const float4 ay4 = *reinterpret_cast<const float4 *>(ry + 4 * r4);
+                    const float4 cx0 = *reinterpret_cast<const float4 *>(rx + 8 * c8);
+                    const float4 cx1 = *reinterpret_cast<const float4 *>(rx + 8 * c8 + 4);
+                    const float4 cy0 = *reinterpret_cast<const float4 *>(ry + 8 * c8);
+                    const float4 cy1 = *reinterpret_cast<const float4 *>(ry + 8 * c8 + 4);
+                    const double axv[4] = {ax4.x, ax4.y, ax4.z, ax4.w}, ayv[4] = {ay4.x, ay4.y, ay4.z, ay4.w};
+                    const double cxv[8] = {cx0.x, cx0.y, cx0.z, cx0.w, cx1.x, cx1.y, cx1.z, cx1.w};
+                    const double cyv[8] = {cy0.x, cy0.y, cy0.z, cy0.w, cy1.x, cy1.y, cy1.z, cy1.w};
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(ayv[i], cyv[j], fma(axv[i], cxv[j], acc[i][j]));
+                        for (int j = 0; j < 8; ++j) acc[i][j] = fma(ayv[i], cyv[j], fma(axv[i], cxv[j], acc[i][j]));
                 }
-            }
-            if (tid < KTP) {
+            } else if (gthread) {
                 for (int q = 0; q < cn; ++q) {
                     const int qc = it * NE_SUB + q;
-                    gacc = fma(hd.w[2 * qc + 1], rows[(2 * q + 1) * KTP + tid], fma(hd.w[2 * qc], rows[(2 * q) * KTP + tid], gacc));
+                    gacc = fma(hd.w[2 * qc + 1], (double)rows[(2 * q + 1) * KTP + gcol],
+                               fma(hd.w[2 * qc], (double)rows[(2 * q) * KTP + gcol], gacc));
                 }
             }
         }
         double *part = b.ne_part + ((size_t)f * NE_MAXCH + ch) * stride;
-        if (bi >= 0) {
-            double2 *o = reinterpret_cast<double2 *>(part + tid * 16);
+        if (r4 >= 0) {
+            double2 *o = reinterpret_cast<double2 *>(part + tid * 32);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                o[2 * i] = make_double2(acc[i][0], acc[i][1]);
-                o[2 * i + 1] = make_double2(acc[i][2], acc[i][3]);
-            }
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; j += 2) o[(i * 8 + j) / 2] = make_double2(acc[i][j], acc[i][j + 1]);
         }
-        if (tid < KTP) part[nb4 * (nb4 + 1) / 2 * 16 + tid] = gacc;
+        if (gthread) part[NE_TILES * 32 + gcol] = gacc;
     }
 }
 
@@ -1455,39 +1459,38 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatc
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     const int KTP = m.KTP, KT = m.KT, tid = threadIdx.x;
-    const int nb4 = KTP / 4;
     const int stride = ne_part_stride(KTP);
     const int nch = (ctl.N + NE_CH - 1) / NE_CH;
     const double *part = b.ne_part + (size_t)f * NE_MAXCH * stride;
     const double tau = 25.0;
     float *H = b.H + (size_t)f * KTP * KTP;
-    int bi, bj;
-    ne_block(tid, nb4, bi, bj);
-    if (bi >= 0) {
-        double s[16];
+    int r4, c8;
+    ne_tile(tid, r4, c8);
+    if (r4 >= 0) {
+        double s[32];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) s[e] = 0.0;
+        for (int e = 0; e < 32; ++e) s[e] = 0.0;
         for (int q = 0; q < nch; ++q) {
-            const double2 *p = reinterpret_cast<const double2 *>(part + (size_t)q * stride + tid * 16);
+            const double2 *p = reinterpret_cast<const double2 *>(part + (size_t)q * stride + tid * 32);
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
+            for (int e = 0; e < 16; ++e) {
                 const double2 v = p[e];
                 s[2 * e] += v.x;
                 s[2 * e + 1] += v.y;
             }
         }
         for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 4; ++j) {
-                const int a = 4 * bi + i, c = 4 * bj + j;
-                if (a >= KT || c >= KT) continue;
-                const float v = (float)(tau * s[i * 4 + j]);
+            for (int j = 0; j < 8; ++j) {
+                const int a = 4 * r4 + i, c = 8 * c8 + j;
+                if (a > c || c >= KT) continue;
+                const float v = (float)(tau * s[i * 8 + j]);
                 H[(size_t)a * KTP + c] = v;
                 H[(size_t)c * KTP + a] = v;
             }
     }
     if (tid < KT) {
         double s = 0.0;
-        for (int q = 0; q < nch; ++q) s += part[(size_t)q * stride + nb4 * (nb4 + 1) / 2 * 16 + tid];
+        for (int q = 0; q < nch; ++q) s += part[(size_t)q * stride + NE_TILES * 32 + tid];
         b.g[(size_t)f * KTP + tid] = (float)(-tau * s);
     }
 }
