@@ -309,7 +309,7 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
         else
             TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq_tc<TC_MAXN / 8>, dim3(TC_BPF, L.A()), dim3(TC_THREADS),
                            (size_t)TC_SMEM, L.s, L.m, L.b));
-        TDI_TRY(launch(L.bt, 0, k_normal_eq_tc_reduce, dim3(L.A()), dim3(256), 0, L.s, L.m, L.b));
+        TDI_TRY(launch(L.bt, 0, k_normal_eq_tc_reduce, dim3(TC_RBLOCKS, L.A()), dim3(256), 0, L.s, L.m, L.b));
     } else {
         TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_BPF, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
         TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));

@@ -1470,14 +1470,23 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatc
         double s[32];
 #pragma unroll
         for (int e = 0; e < 32; ++e) s[e] = 0.0;
+        // the next chunk's values are loaded while this chunk's are added
+        const double2 *p0 = reinterpret_cast<const double2 *>(part + tid * 32);
+        double2 cur[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) cur[e] = nch > 0 ? p0[e] : make_double2(0.0, 0.0);
         for (int q = 0; q < nch; ++q) {
-            const double2 *p = reinterpret_cast<const double2 *>(part + (size_t)q * stride + tid * 32);
+            double2 nxt[16];
+            const double2 *pn = reinterpret_cast<const double2 *>(part + (size_t)(q + 1) * stride + tid * 32);
+#pragma unroll
+            for (int e = 0; e < 16; ++e) nxt[e] = q + 1 < nch ? pn[e] : make_double2(0.0, 0.0);
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
-                const double2 v = p[e];
-                s[2 * e] += v.x;
-                s[2 * e + 1] += v.y;
+                s[2 * e] += cur[e].x;
+                s[2 * e + 1] += cur[e].y;
             }
+#pragma unroll
+            for (int e = 0; e < 16; ++e) cur[e] = nxt[e];
         }
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 8; ++j) {

@@ -253,9 +253,13 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_normal_eq_tc(DModel m, DBatch
 }
 
 // H = tau * (sum over chunks, in order, of the chunk sums) in FP64; g from the weight column.
+// TC_RBLOCKS blocks per frame, each over a slice of the entries; the chunk values of an entry
+// are loaded eight at a time.
+constexpr int TC_RBLOCKS = 4;
+
 __global__ void __launch_bounds__(256) k_normal_eq_tc_reduce(DModel m, DBatch b)
 {
-    const int f = b.act[blockIdx.x];
+    const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     const int KTP = m.KTP, KT = m.KT, PK = tc_pitch(KT);
@@ -265,11 +269,20 @@ __global__ void __launch_bounds__(256) k_normal_eq_tc_reduce(DModel m, DBatch b)
     const double tau = 25.0;
     float *H = b.H + (size_t)f * KTP * KTP;
     // entry (a, c), a <= c <= KT, sits at [c][a]; consecutive threads take consecutive a
-    for (int e = threadIdx.x; e < (KT + 1) * PK; e += blockDim.x) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (KT + 1) * PK; e += gridDim.x * blockDim.x) {
         const int c = e / PK, a = e - c * PK;
         if (a > c) continue;
+        const float *p = base + (size_t)c * PK + a;
         double s = 0.0;
-        for (int q = 0; q < nch; ++q) s += (double)base[(size_t)q * pstride + (size_t)c * PK + a];
+        int q = 0;
+        for (; q + 8 <= nch; q += 8) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = p[(size_t)(q + u) * pstride];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s += (double)v[u];
+        }
+        for (; q < nch; ++q) s += (double)p[(size_t)q * pstride];
         if (c < KT) {
             const float v = (float)(tau * s);
             H[(size_t)a * KTP + c] = v;

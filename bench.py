@@ -129,9 +129,11 @@ def measured_peaks():
 def algorithmic_bytes(kernel: str, V: int, T: int, K: int, n_frag: float):
     """(bytes per frame, bytes per launch) a kernel must move: what the roofline divides by."""
     if kernel == "vertex":
-        # outputs per frame (object coordinates 12 B, projection 16 B per vertex) and the
-        # coefficients; the basis (3*V*K*4 B) once per launch, shared by all its frames
-        return 28.0 * V + 4.0 * K, 12.0 * V * K
+        # outputs per frame (object coordinates 12 B, projection x, y, Z 12 B per vertex) and
+        # the coefficients; the basis (3*V*K*4 B) once per launch, shared by all its frames.
+        # The stored records are two float4 per vertex (32 B): padding and the albedo copy
+        # are not counted as algorithmic bytes.
+        return 24.0 * V + 4.0 * K, 12.0 * V * K
     if kernel == "raster":
         # depth pass: projections (16 B per vertex), triangle corners and visiting order
         # (16 B per triangle), one 8-byte depth key per visible fragment
