@@ -130,10 +130,24 @@ struct tdi_model {
     int device = 0;
 };
 
+// A lane is a contiguous range of a batch's frames with its own stream and active-frame count:
+// the fit runs its lanes' round loops side by side, so that the kernels of one lane fill the
+// SMs that the other lane's per-frame kernels leave idle.
+struct tdi_lane {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    int *d_count = nullptr;        // [2]: active frames, error word
+    int *h_count = nullptr;        // pinned copy
+    DBatch d{};                    // view of the lane's frames
+    int n = 0;                     // frames running the current stage
+};
+
 struct tdi_batch {
     tdi_model *m = nullptr;
     int cap = 0;
     DBatch d{};
+    std::vector<tdi_lane> lanes;
+    size_t ne_frame_doubles = 0;   // per-frame extent of d.ne_part
     std::vector<void *> allocs;
     float *target_raw = nullptr;   // [cap][NPIX] unblurred upload
     float *ctrl_scratch = nullptr;
@@ -147,6 +161,9 @@ struct tdi_batch {
 };
 
 namespace {
+
+constexpr int FIT_LANES = 2;       // streams a batched fit runs on
+constexpr int FIT_LANE_MIN = 32;   // frames a lane needs before a batch is split
 
 template <typename T>
 tdi_status dalloc(std::vector<void *> &list, T **p, size_t n)
@@ -267,6 +284,62 @@ struct Launch {
     dim3 ablocks() const { return dim3((A() + 127) / 128); }
 };
 
+// View of frames [f0, f0 + nf) of a batch: every per-frame array starts at frame f0.
+DBatch batch_view(const tdi_batch *bt, int f0, int nf)
+{
+    const DModel &m = bt->m->d;
+    const DBatch &a = bt->d;
+    const size_t F0 = (size_t)f0, KTP = m.KTP;
+    DBatch v = a;
+    v.F = nf;
+    v.target = a.target + F0 * NPIX;
+    v.xl = a.xl + F0 * NL; v.yl = a.yl + F0 * NL;
+    v.bounds = a.bounds + F0 * 4 * NL;
+    v.face_size = a.face_size + F0;
+    v.cam = a.cam + F0 * 4;
+    v.x0y0 = a.x0y0 + F0 * 2;
+    v.Lint = a.Lint + F0;
+    v.x = a.x + F0 * KTP; v.x_ls = a.x_ls + F0 * KTP; v.xe = a.xe + F0 * KTP;
+    v.lam = a.lam + F0 * 4; v.lam_ls = a.lam_ls + F0 * 4; v.lame = a.lame + F0 * 4;
+    v.dlam = a.dlam + F0 * 4; v.glam = a.glam + F0 * 4;
+    v.d = a.d + F0 * KTP; v.g = a.g + F0 * KTP;
+    v.H = a.H + F0 * KTP * KTP;
+    v.R = a.R + F0 * 9; v.dR = a.dR + F0 * 27;
+    v.ctl = a.ctl + F0;
+    v.act = a.act + F0;
+    v.nact = 0;
+    v.geo = a.geo + F0 * m.V; v.proj = a.proj + F0 * m.V;
+    v.zbuf = a.zbuf + F0 * NPIX;
+    v.tri_mask = a.tri_mask + F0 * mask_words(m.T);
+    v.tri_list = a.tri_list + F0 * m.T;
+    v.frag = a.frag + F0 * NMAX;
+    v.fgrad = a.fgrad + F0 * 5 * NMAX;
+    v.nb = a.nb + F0 * 4 * NMAX;
+    v.perm = a.perm + F0 * NMAX;
+    v.J = a.J + F0 * NMAX * KTP;
+    v.ne_part = a.ne_part + F0 * bt->ne_frame_doubles;
+    v.img = a.img + F0 * 2 * NPIX;
+    return v;
+}
+
+// Compacts a lane's list of frames running the stage; the count arrives with the lane's
+// next synchronisation (one 8-byte read-back per round and lane).
+tdi_status lane_compact(tdi_batch *bt, tdi_lane &ln)
+{
+    TDI_TRY(launch(bt, 0, k_compact_active, dim3(1), dim3(1024), 0, ln.s, (const DBatch)ln.d, ln.d_count));
+    TDI_CUDA(cudaMemcpyAsync(ln.h_count, ln.d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, ln.s));
+    return TDI_OK;
+}
+
+tdi_status lane_count(tdi_lane &ln)
+{
+    TDI_CUDA(cudaStreamSynchronize(ln.s));
+    if (ln.h_count[1]) return fail(TDI_ERR_CUDA, "a bounded device-side wait gave up (error word set)");
+    ln.n = ln.h_count[0];
+    ln.d.nact = ln.n;
+    return TDI_OK;
+}
+
 // Compacts the list of frames running the stage and returns how many there are (one 4-byte
 // read-back per call).
 tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
@@ -320,33 +393,54 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
     return TDI_OK;
 }
 
-tdi_status run_stage(tdi_batch *bt, const Cfg &c, int stage, cudaStream_t s)
+// One round of a stage for the frames of b (launched on s).
+tdi_status stage_round(tdi_batch *bt, const Cfg &c, int stage, const DBatch &b, cudaStream_t s, long round)
 {
     const DModel &m = bt->m->d;
-    const DBatch &b = bt->d;
     Launch L{bt, m, b, s, b.F};
-    TDI_TRY(launch(bt, 0, k_stage_start, L.fblocks(), dim3(128), 0, s, m, b, c, stage));
-    int n = 0;
-    TDI_TRY(compact_active(bt, s, &n));
+    TDI_TRY(launch(bt, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, b, stage));
+    if (stage == ST_LAMBDA) {
+        if (round == 0) {
+            TDI_TRY(geometry(L, c, stage));
+            TDI_TRY(launch(bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), s, b, 1));
+        }
+        TDI_TRY(render(L, c, stage));
+        TDI_TRY(launch(bt, 0, k_decide_lambda, L.ablocks(), dim3(128), 0, s, m, b, c));
+        TDI_TRY(launch(bt, 0, k_lambda_jac, dim3(L.A()), dim3(256), 0, s, m, b, c));
+    } else {
+        TDI_TRY(geometry(L, c, stage));
+        TDI_TRY(render(L, c, stage));
+        TDI_TRY(launch(bt, 0, k_decide_shape, L.ablocks(), dim3(128), 0, s, m, b, c, stage));
+        TDI_TRY(normal_equations(L, c, stage));
+    }
+    return TDI_OK;
+}
+
+// A stage (fit_3DMM_lambdas / _shape_rigid / _epsilon_finetune) for every frame of every lane:
+// the lanes' rounds are enqueued on their own streams before any lane is waited for.
+tdi_status run_stage_lanes(tdi_batch *bt, const Cfg &c, int stage, int nlanes)
+{
+    const DModel &m = bt->m->d;
+    for (int l = 0; l < nlanes; ++l) {
+        tdi_lane &ln = bt->lanes[l];
+        TDI_TRY(launch(bt, 0, k_stage_start, dim3((ln.d.F + 127) / 128), dim3(128), 0, ln.s, m, ln.d, c, stage));
+        TDI_TRY(lane_compact(bt, ln));
+    }
+    for (int l = 0; l < nlanes; ++l) TDI_TRY(lane_count(bt->lanes[l]));
     const long max_rounds = stage == ST_LAMBDA ? 8L * c.max_iters_lambda + 16
                                                : 16L * (stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune) + 16;
-    for (long round = 0; round < max_rounds && n > 0; ++round) {
-        TDI_TRY(launch(bt, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, b, stage));
-        if (stage == ST_LAMBDA) {
-            if (round == 0) {
-                TDI_TRY(geometry(L, c, stage));
-                TDI_TRY(launch(bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), s, b, 1));
-            }
-            TDI_TRY(render(L, c, stage));
-            TDI_TRY(launch(bt, 0, k_decide_lambda, L.ablocks(), dim3(128), 0, s, m, b, c));
-            TDI_TRY(launch(bt, 0, k_lambda_jac, dim3(L.A()), dim3(256), 0, s, m, b, c));
-        } else {
-            TDI_TRY(geometry(L, c, stage));
-            TDI_TRY(render(L, c, stage));
-            TDI_TRY(launch(bt, 0, k_decide_shape, L.ablocks(), dim3(128), 0, s, m, b, c, stage));
-            TDI_TRY(normal_equations(L, c, stage));
+    for (long round = 0; round < max_rounds; ++round) {
+        bool any = false;
+        for (int l = 0; l < nlanes; ++l) {
+            tdi_lane &ln = bt->lanes[l];
+            if (ln.n <= 0) continue;
+            any = true;
+            TDI_TRY(stage_round(bt, c, stage, ln.d, ln.s, round));
+            TDI_TRY(lane_compact(bt, ln));
         }
-        TDI_TRY(compact_active(bt, s, &n));
+        if (!any) break;
+        for (int l = 0; l < nlanes; ++l)
+            if (bt->lanes[l].n > 0) TDI_TRY(lane_count(bt->lanes[l]));
     }
     return TDI_OK;
 }
@@ -524,7 +618,8 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
     A(d.ctl, F); A(d.act, F); A(d.geo, F * (size_t)md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
-    A(d.J, F * NMAX * KTP); A(d.ne_part, F * NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8)); A(d.err, 1); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 2);
+    A(d.J, F * NMAX * KTP); b->ne_frame_doubles = NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8);
+    A(d.ne_part, F * b->ne_frame_doubles); A(d.err, 1); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 2);
     A(d.prof_frames, 1);
 #undef A
     if (st != TDI_OK) return cleanup(st);
@@ -542,6 +637,17 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     d.target = target; d.xl = xl; d.yl = yl; d.bounds = bounds; d.face_size = fs; d.cam = cam;
     d.x0y0 = x0y0; d.Lint = Lint;
     d.prof_id = 0;
+    // lanes: two for batches that can be halved, each with a non-blocking stream
+    b->lanes.resize(max_frames >= 2 ? FIT_LANES : 1);
+    for (auto &ln : b->lanes) {
+        if (cudaStreamCreateWithFlags(&ln.s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ln.ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost(&ln.h_count, 2 * sizeof(int)) != cudaSuccess ||
+            dalloc(b->allocs, &ln.d_count, 2) != TDI_OK) {
+            tdi_batch_destroy(b);
+            return fail(TDI_ERR_CUDA, "lane creation failed");
+        }
+    }
     *out = b;
     return TDI_OK;
 }
@@ -550,6 +656,11 @@ tdi_status tdi_batch_destroy(tdi_batch *b)
 {
     if (!b) return TDI_OK;
     for (auto &e : b->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    for (auto &ln : b->lanes) {
+        if (ln.s) cudaStreamDestroy(ln.s);
+        if (ln.ev) cudaEventDestroy(ln.ev);
+        if (ln.h_count) cudaFreeHost(ln.h_count);
+    }
     for (void *p : b->allocs) cudaFree(p);
     if (b->h_count) cudaFreeHost(b->h_count);
     delete b;
@@ -623,15 +734,29 @@ tdi_status tdi_batch_fit(tdi_batch *b, const tdi_fit_config *cfg, void *stream)
     const dim3 fb((b->d.F + 127) / 128);
     TDI_TRY(blur_targets(b, c, s));
     TDI_TRY(launch(b, 0, k_fit_begin, fb, dim3(128), 0, s, b->d));
-    TDI_TRY(run_stage(b, c, ST_LAMBDA, s));
-    TDI_TRY(run_stage(b, c, ST_RIGID, s));
+    // lanes: halves of the batch on their own streams, ordered after the work on s
+    const int F = b->d.F;
+    const int nlanes = std::min((int)b->lanes.size(), F >= 2 * FIT_LANE_MIN ? FIT_LANES : 1);
+    TDI_CUDA(cudaEventRecord(b->lanes[0].ev, s));
+    for (int l = 0; l < nlanes; ++l) {
+        tdi_lane &ln = b->lanes[l];
+        const int f0 = (int)((long)F * l / nlanes), f1 = (int)((long)F * (l + 1) / nlanes);
+        ln.d = batch_view(b, f0, f1 - f0);
+        TDI_CUDA(cudaStreamWaitEvent(ln.s, b->lanes[0].ev, 0));
+    }
+    TDI_TRY(run_stage_lanes(b, c, ST_LAMBDA, nlanes));
+    TDI_TRY(run_stage_lanes(b, c, ST_RIGID, nlanes));
     if (c.twostage_illum) {
         for (int k = 0; k < 2; ++k) {
-            TDI_TRY(run_stage(b, c, ST_LAMBDA, s));
-            TDI_TRY(run_stage(b, c, ST_RIGID, s));
+            TDI_TRY(run_stage_lanes(b, c, ST_LAMBDA, nlanes));
+            TDI_TRY(run_stage_lanes(b, c, ST_RIGID, nlanes));
         }
     }
-    if (c.finetune) TDI_TRY(run_stage(b, c, ST_FINETUNE, s));
+    if (c.finetune) TDI_TRY(run_stage_lanes(b, c, ST_FINETUNE, nlanes));
+    for (int l = 0; l < nlanes; ++l) {
+        TDI_CUDA(cudaEventRecord(b->lanes[l].ev, b->lanes[l].s));
+        TDI_CUDA(cudaStreamWaitEvent(s, b->lanes[l].ev, 0));
+    }
     TDI_TRY(launch(b, 0, k_fit_end, fb, dim3(128), 0, s, b->d));
     return TDI_OK;
 }
