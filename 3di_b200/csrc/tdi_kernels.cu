@@ -1519,6 +1519,7 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     float *Fm = bsm;                              // [4*NL][KTP]
     __shared__ float G[4][NL];
     __shared__ float s_p[NL][3];
+    __shared__ float s_v[NL][3], s_ivz[NL], s_ivz2[NL];
     const int tid = threadIdx.x;
     const float *x = b.x + (size_t)f * KTP;       // the accepted point (= evaluation point)
     const float *R = b.R + f * 9, *dR = b.dR + f * 27;
@@ -1543,16 +1544,20 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
         G[1][tid] = 0.0f - ((yl[tid] + bnd[1 * NL + tid] * fs) - yproj);
         G[2][tid] = 0.0f - ((xproj - bnd[2 * NL + tid] * fs) - xl[tid]);
         G[3][tid] = 0.0f - ((yproj - bnd[3 * NL + tid] * fs) - yl[tid]);
+        // camera point of the landmark and its inverse depth, once per landmark
+        const float vx = r1p + tau[0], vy = r2p + tau[1], vz = r3p + tau[2];
+        s_v[tid][0] = vx; s_v[tid][1] = vy; s_v[tid][2] = vz;
+        const float ivz = 1.0f / vz;
+        s_ivz[tid] = ivz;
+        s_ivz2[tid] = ivz * ivz;
     }
     __syncthreads();
-    for (int idx = tid; idx < NL * KTP; idx += 256) {
-        const int i = idx / KTP, a = idx - i * KTP;
+    // rows of the constraint gradients: warps take landmarks, lanes take columns
+    for (int i = tid >> 5; i < NL; i += 8)
+    for (int a = tid & 31; a < KTP; a += 32) {
         const float p0 = s_p[i][0], p1 = s_p[i][1], p2 = s_p[i][2];
-        const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
-        const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
-        const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
-        const float vx = r1p + tau[0], vy = r2p + tau[1], vz = r3p + tau[2];
-        const float ivz = 1.0f / vz, ivz2 = ivz * ivz;
+        const float vx = s_v[i][0], vy = s_v[i][1], vz = s_v[i][2];
+        const float ivz = s_ivz[i], ivz2 = s_ivz2[i];
         float wx = 0.0f, wy = 0.0f;
         if (a < K) {
             const float *ex = m.E + (size_t)m.lis[i] * 3 * m.KP;
@@ -1601,27 +1606,47 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
         }
         gv[a] += ga;
     }
-    // Hessian: lower triangle entries (a >= c), mirrored
-    const int npairs = KT * (KT + 1) / 2;
-    for (int pidx = tid; pidx < npairs; pidx += 256) {
-        int a = (int)((sqrtf(8.0f * (float)pidx + 1.0f) - 1.0f) * 0.5f);
-        while ((a + 1) * (a + 2) / 2 <= pidx) ++a;
-        while (a * (a + 1) / 2 > pidx) --a;
-        const int c = pidx - a * (a + 1) / 2;
-        double hs = 0.0;
-        for (int s = 0; s < 4; ++s)
-            for (int i = 0; i < NL; ++i)
-                hs += (double)Fm[(s * NL + i) * KTP + a] * (double)Fm[(s * NL + i) * KTP + c];
-        float hv = (float)hs;
-        if (a == c && a < K) {
-            const float fub = x[a] - ub[a];
-            const float flb = lb[a] - x[a];
-            const float nu = (float)(-1.0 / ((double)fub + 1e-12));
-            const float nl = (float)(1.0 / ((double)flb + 1e-12));
-            hv = hv + (nu * nu + nl * nl);
+    // Hessian: 4 x 8 tiles of the upper triangle (NE_TILES threads), each entry summed in FP64
+    // over the constraints in the oracle's order (set, then landmark), mirrored. The terms are
+    // products of floats, exact in FP64, so the fused multiply-add rounds like the oracle's
+    // multiply-then-add.
+    int r4, c8;
+    ne_tile(tid, r4, c8);
+    if (r4 >= 0) {
+        double acc[4][8];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+        for (int t = 0; t < 4 * NL; ++t) {
+            const float *row = Fm + (size_t)t * KTP;
+            const float4 a4 = *reinterpret_cast<const float4 *>(row + 4 * r4);
+            const float4 c0 = *reinterpret_cast<const float4 *>(row + 8 * c8);
+            const float4 c1 = *reinterpret_cast<const float4 *>(row + 8 * c8 + 4);
+            const double av[4] = {a4.x, a4.y, a4.z, a4.w};
+            const double cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], cv[j], acc[i][j]);
         }
-        H[(size_t)a * KTP + c] += hv;
-        if (a != c) H[(size_t)c * KTP + a] += hv;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int a = 4 * r4 + i, c = 8 * c8 + j;
+                if (a > c || c >= KT) continue;
+                float hv = (float)acc[i][j];
+                if (a == c && a < K) {
+                    const float fub = x[a] - ub[a];
+                    const float flb = lb[a] - x[a];
+                    const float nu = (float)(-1.0 / ((double)fub + 1e-12));
+                    const float nl = (float)(1.0 / ((double)flb + 1e-12));
+                    hv = hv + (nu * nu + nl * nl);
+                }
+                H[(size_t)c * KTP + a] += hv;
+                if (a != c) H[(size_t)a * KTP + c] += hv;
+            }
     }
 }
 
