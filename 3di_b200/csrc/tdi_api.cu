@@ -101,8 +101,8 @@ tdi_status check_cfg(const tdi_fit_config &c, const DModel &m)
     if (c.normal_eq != 0 && c.normal_eq != 1) return fail(TDI_ERR_INVALID, "normal_eq must be 0 or 1");
     if (c.normal_eq == 1 && m.KT + 1 > TC_MAXN)
         return fail(TDI_ERR_INVALID, "tensor-core normal equations take at most 121 expression components");
-    if (c.normal_eq == 0 && m.KTP > 8 * NE_GRP)
-        return fail(TDI_ERR_INVALID, "exact normal equations take at most 82 expression components");
+    if (c.normal_eq == 0 && m.KT + 1 > NE_P8)
+        return fail(TDI_ERR_INVALID, "exact normal equations take at most 81 expression components");
     return TDI_OK;
 }
 
@@ -276,7 +276,7 @@ struct Launch {
     int F;
     size_t smem_vertex() const { return vt_smem(m.KP); }
     size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
-    size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * m.KTP * sizeof(float); }
+    size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * NE_P8 * sizeof(float); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
     size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
     dim3 fblocks() const { return dim3((F + 127) / 128); }
@@ -385,7 +385,7 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
         TDI_TRY(launch(L.bt, 0, k_normal_eq_tc_reduce, dim3(TC_RBLOCKS, L.A()), dim3(256), 0, L.s, L.m, L.b));
     } else {
         TDI_TRY(launch(L.bt, KID_NORMAL_EQ, k_normal_eq, dim3(NE_BPF, L.A()), dim3(NE_THREADS), L.smem_ne(), L.s, L.m, L.b));
-        TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));
+        TDI_TRY(launch(L.bt, 0, k_normal_eq_reduce, dim3(4, L.A()), dim3(NE_THREADS), 0, L.s, L.m, L.b));
     }
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));

@@ -1297,7 +1297,7 @@ __device__ __forceinline__ void ne_tile(int t, int &r4, int &c8)
 
 __host__ __device__ __forceinline__ int ne_part_stride(int KTP)
 {
-    return NE_TILES * 32 + KTP;
+    return NE_TILES * 32 + KTP;   // the widest partial layout of the normal-equation kernels
 }
 
 // Rows of one chunk of NE_CH fragments: per-fragment scalars and neighbour indices are
@@ -1360,43 +1360,68 @@ __device__ __forceinline__ void chain_value(const float (&vv)[4], float pre, flo
     oy = (pre * (-diffx)) * X;
 }
 
+// FP64 tensor-core form of the exact sum: mma.sync m8n8k4 f64 updates an 8x8 tile with four
+// rows k = 0..3 as the fused multiply-add chain d = fma(a3, b3, fma(a2, b2, fma(a1, b1,
+// fma(a0, b0, c)))) (checked on B200 against CPU emulation: no mismatch in 4.2M entries; the
+// parity tests check H and g bit for bit). Four rows are two fragments' x and y rows in
+// order, so the chain is exactly the oracle's. Tiles of 8x8 cover the upper triangle of a
+// P8 x P8 matrix whose column KT holds the weights w (so the column KT of the sum is g).
+constexpr int NE_P8 = 88;                    // padded width: parameters + weight column, <= 88
+constexpr int NE_T8 = NE_P8 / 8;             // 11 tile rows / columns
+constexpr int NE_NT8 = NE_T8 * (NE_T8 + 1) / 2;   // 66 tiles
+constexpr int NE_TPW = (NE_NT8 + 7) / 8;     // tiles per warp (8 warps)
+
+__device__ __forceinline__ void ne_tile8(int t, int &bi, int &bj)
+{
+    bi = 0;
+    while (t >= NE_T8 - bi) { t -= NE_T8 - bi; ++bi; }
+    bj = bi + t;
+}
+
+__host__ __device__ __forceinline__ int ne_part_stride8() { return NE_NT8 * 64; }
+
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
 __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
 {
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
-    extern __shared__ __align__(16) float nesf[];   // rows [2][2*NE_SUB][KTP], FP32
+    extern __shared__ __align__(16) float nesf[];   // rows [2][2*NE_SUB][NE_P8], FP32
     const int KTP = m.KTP, KT = m.KT;
     __shared__ ChunkHead hd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int a_low = lane & 7, q_me = 4 * warp + (lane >> 3);
-    // threads below NE_TILES own a 4 x 8 tile of the sum; the next KTP threads own one entry
-    // of the weighted sum; both work on the stage the build has just finished
-    int r4, c8;
-    ne_tile(tid, r4, c8);
-    const int gcol = tid - NE_TILES;
-    const bool gthread = gcol >= 0 && gcol < KTP;
     const int N = ctl.N;
     const int nch = (N + NE_CH - 1) / NE_CH;
     const float *Jf = b.J + (size_t)f * NMAX * KTP;
     const int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
     const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
-    const int stride = ne_part_stride(KTP);
+    const int stride = ne_part_stride8();
+    // this warp's tiles: t = warp + 8 * j
+    int tbi[NE_TPW], tbj[NE_TPW];
+#pragma unroll
+    for (int j = 0; j < NE_TPW; ++j) {
+        const int t = warp + 8 * j;
+        if (t < NE_NT8) ne_tile8(t, tbi[j], tbj[j]); else { tbi[j] = -1; tbj[j] = -1; }
+    }
+    const int kr = lane & 3, fr8 = lane >> 2;        // fragment row k and tile row/column
     for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        double acc[4][8];
+        double acc[NE_TPW][2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-        double gacc = 0.0;
+        for (int j = 0; j < NE_TPW; ++j) acc[j][0] = acc[j][1] = 0.0;
         const int c0 = ch * NE_CH, cnt = min(N, c0 + NE_CH) - c0;
         const int nsub = (cnt + NE_SUB - 1) / NE_SUB;
         __syncthreads();                          // the previous chunk is done with hd and the rows
         chunk_head(hd, fg, nb, c0, cnt);
         __syncthreads();
         for (int it = 0; it < nsub; ++it) {
-            float *rows = nesf + (size_t)(it & 1) * 2 * NE_SUB * KTP;
+            float *rows = nesf + (size_t)(it & 1) * 2 * NE_SUB * NE_P8;
             {
                 float v[NE_GRP][4];
                 const int ql = q_me, q = it * NE_SUB + ql;
@@ -1406,101 +1431,90 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
 #pragma unroll
                 for (int g = 0; g < NE_GRP; ++g) {
                     const int a = 8 * g + a_low;
-                    if (a >= KTP) continue;
+                    if (a >= NE_P8) continue;
                     float ox = 0.0f, oy = 0.0f;
-                    if (live && a < KT) chain_value(v[g], pre, diffx, diffy, ox, oy);
-                    rows[(2 * ql) * KTP + a] = ox;
-                    rows[(2 * ql + 1) * KTP + a] = oy;
+                    if (live) {
+                        if (a < KT) chain_value(v[g], pre, diffx, diffy, ox, oy);
+                        else if (a == KT) { ox = (float)hd.w[2 * q]; oy = (float)hd.w[2 * q + 1]; }
+                    }
+                    rows[(2 * ql) * NE_P8 + a] = ox;
+                    rows[(2 * ql + 1) * NE_P8 + a] = oy;
                 }
             }
             __syncthreads();
             const int cn = min(NE_SUB, cnt - it * NE_SUB);
-            if (r4 >= 0) {
-                for (int q = 0; q < cn; ++q) {
-                    const float *rx = rows + (2 * q) * KTP, *ry = rx + KTP;
-                    const float4 ax4 = *reinterpret_cast<const float4 *>(rx + 4 * r4);
-                    const float4 ay4 = *reinterpret_cast<const float4 *>(ry + 4 * r4);
-                    const float4 cx0 = *reinterpret_cast<const float4 *>(rx + 8 * c8);
-                    const float4 cx1 = *reinterpret_cast<const float4 *>(rx + 8 * c8 + 4);
-                    const float4 cy0 = *reinterpret_cast<const float4 *>(ry + 8 * c8);
-                    const float4 cy1 = *reinterpret_cast<const float4 *>(ry + 8 * c8 + 4);
-                    const double axv[4] = {ax4.x, ax4.y, ax4.z, ax4.w}, ayv[4] = {ay4.x, ay4.y, ay4.z, ay4.w};
-                    const double cxv[8] = {cx0.x, cx0.y, cx0.z, cx0.w, cx1.x, cx1.y, cx1.z, cx1.w};
-                    const double cyv[8] = {cy0.x, cy0.y, cy0.z, cy0.w, cy1.x, cy1.y, cy1.z, cy1.w};
+            // pairs of fragments on the tensor cores
+            for (int q = 0; q + 2 <= cn; q += 2) {
+                const float *rk = rows + (size_t)(2 * q + kr) * NE_P8;
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[i][j] = fma(ayv[i], cyv[j], fma(axv[i], cxv[j], acc[i][j]));
+                for (int j = 0; j < NE_TPW; ++j) {
+                    if (tbi[j] < 0) continue;
+                    const double av = (double)rk[8 * tbi[j] + fr8];
+                    const double bv = (double)rk[8 * tbj[j] + fr8];
+                    dmma_884(acc[j][0], acc[j][1], av, bv);
                 }
-            } else if (gthread) {
-                for (int q = 0; q < cn; ++q) {
-                    const int qc = it * NE_SUB + q;
-                    gacc = fma(hd.w[2 * qc + 1], (double)rows[(2 * q + 1) * KTP + gcol],
-                               fma(hd.w[2 * qc], (double)rows[(2 * q) * KTP + gcol], gacc));
+            }
+            // an odd last fragment: this thread's two entries of each tile, same chain
+            if (cn & 1) {
+                const int q = cn - 1;
+                const float *rx = rows + (size_t)(2 * q) * NE_P8, *ry = rx + NE_P8;
+#pragma unroll
+                for (int j = 0; j < NE_TPW; ++j) {
+                    if (tbi[j] < 0) continue;
+                    const int r = 8 * tbi[j] + fr8, c = 8 * tbj[j] + 2 * kr;
+#pragma unroll
+                    for (int i = 0; i < 2; ++i)
+                        acc[j][i] = fma((double)ry[r], (double)ry[c + i], fma((double)rx[r], (double)rx[c + i], acc[j][i]));
                 }
             }
         }
         double *part = b.ne_part + ((size_t)f * NE_MAXCH + ch) * stride;
-        if (r4 >= 0) {
-            double2 *o = reinterpret_cast<double2 *>(part + tid * 32);
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; j += 2) o[(i * 8 + j) / 2] = make_double2(acc[i][j], acc[i][j + 1]);
+        for (int j = 0; j < NE_TPW; ++j) {
+            if (tbi[j] < 0) continue;
+            const int t = warp + 8 * j;
+            *reinterpret_cast<double2 *>(part + t * 64 + fr8 * 8 + 2 * kr) = make_double2(acc[j][0], acc[j][1]);
         }
-        if (gthread) part[NE_TILES * 32 + gcol] = gacc;
     }
 }
 
-// Sum of the chunk partials in chunk order: H = tau*S, g = -tau*w.
+// Sum of the chunk partials in chunk order: H = tau*S, g = -tau*(column KT of S).
 __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatch b)
 {
-    const int f = b.act[blockIdx.x];
+    const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
-    const int KTP = m.KTP, KT = m.KT, tid = threadIdx.x;
-    const int stride = ne_part_stride(KTP);
+    const int KTP = m.KTP, KT = m.KT;
+    const int stride = ne_part_stride8();
     const int nch = (ctl.N + NE_CH - 1) / NE_CH;
     const double *part = b.ne_part + (size_t)f * NE_MAXCH * stride;
     const double tau = 25.0;
     float *H = b.H + (size_t)f * KTP * KTP;
-    int r4, c8;
-    ne_tile(tid, r4, c8);
-    if (r4 >= 0) {
-        double s[32];
-#pragma unroll
-        for (int e = 0; e < 32; ++e) s[e] = 0.0;
-        // the next chunk's values are loaded while this chunk's are added
-        const double2 *p0 = reinterpret_cast<const double2 *>(part + tid * 32);
-        double2 cur[16];
-#pragma unroll
-        for (int e = 0; e < 16; ++e) cur[e] = nch > 0 ? p0[e] : make_double2(0.0, 0.0);
-        for (int q = 0; q < nch; ++q) {
-            double2 nxt[16];
-            const double2 *pn = reinterpret_cast<const double2 *>(part + (size_t)(q + 1) * stride + tid * 32);
-#pragma unroll
-            for (int e = 0; e < 16; ++e) nxt[e] = q + 1 < nch ? pn[e] : make_double2(0.0, 0.0);
-#pragma unroll
-            for (int e = 0; e < 16; ++e) {
-                s[2 * e] += cur[e].x;
-                s[2 * e + 1] += cur[e].y;
-            }
-#pragma unroll
-            for (int e = 0; e < 16; ++e) cur[e] = nxt[e];
-        }
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < 8; ++j) {
-                const int a = 4 * r4 + i, c = 8 * c8 + j;
-                if (a > c || c >= KT) continue;
-                const float v = (float)(tau * s[i * 8 + j]);
-                H[(size_t)a * KTP + c] = v;
-                H[(size_t)c * KTP + a] = v;
-            }
-    }
-    if (tid < KT) {
+    // one entry per thread: tile t, position p; the chunk values are loaded eight at a time
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < NE_NT8 * 64; e += gridDim.x * blockDim.x) {
+        const int t = e >> 6, pos = e & 63;
+        int bi, bj;
+        ne_tile8(t, bi, bj);
+        const int a = 8 * bi + (pos >> 3), c = 8 * bj + (pos & 7);
+        if (a > c || c > KT || a >= KT) continue;
+        const double *p = part + e;
         double s = 0.0;
-        for (int q = 0; q < nch; ++q) s += part[(size_t)q * stride + NE_TILES * 32 + tid];
-        b.g[(size_t)f * KTP + tid] = (float)(-tau * s);
+        int q = 0;
+        for (; q + 8 <= nch; q += 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = p[(size_t)(q + u) * stride];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s += v[u];
+        }
+        for (; q < nch; ++q) s += p[(size_t)q * stride];
+        if (c < KT) {
+            const float v = (float)(tau * s);
+            H[(size_t)a * KTP + c] = v;
+            H[(size_t)c * KTP + a] = v;
+        } else {
+            b.g[(size_t)f * KTP + a] = (float)(-tau * s);
+        }
     }
 }
 
