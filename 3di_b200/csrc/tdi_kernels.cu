@@ -467,6 +467,39 @@ __device__ __forceinline__ int tri_samples(float bx, float by, float cx, float c
     if (!(denom > 0.0f) && !(denom < 0.0f)) return 0;
     const bool dpos = denom > 0.0f;
     int ridx = 0;
+    // Boxes of at most 2 x 2 sample points (almost every triangle of a dense face mesh): the
+    // same points in the same x-major order, evaluated without loops; at most 4 fragments, so
+    // the NTMP cap cannot bind.
+    if (xhi - xlo_f <= 2.0f && yhi - ylo_f <= 2.0f) {
+        const int xi0 = (int)xlo_f, yi0 = (int)ylo_f;
+#pragma unroll
+        for (int ix = 0; ix < 2; ++ix) {
+            const float xf = xlo_f + (float)ix;
+            if (!(xf < xhi)) break;
+            const float v2x = xf - ax;
+#pragma unroll
+            for (int iy = 0; iy < 2; ++iy) {
+                const float yf = ylo_f + (float)iy;
+                if (!(yf < yhi)) break;
+                const float v2y = yf - ay;
+                const float d20 = v0x * v2x + v0y * v2y;
+                const float d21 = v1x * v2x + v1y * v2y;
+                const float na = d11 * d20 - d01 * d21;
+                const float nb = d00 * d21 - d01 * d20;
+                if ((dpos ? na > 0.0f : na < 0.0f) && (dpos ? nb > 0.0f : nb < 0.0f)) {
+                    const float alpha = na / denom;
+                    const float beta = nb / denom;
+                    if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
+                        const int px = ((yi0 + iy) - y0) + ((xi0 + ix) - x0) * DIM;
+                        if (px < 0 || px >= NPIX) flags |= FLAG_OUT_OF_DOMAIN;
+                        emit(ridx, (uint32_t)(uint16_t)px, alpha, beta);
+                        ridx++;
+                    }
+                }
+            }
+        }
+        return ridx;
+    }
     // Loop counters are kept as floats (integers below 2^24 are exact), which is what the
     // reference's ushort counters are converted to in every comparison and subtraction.
     int xi = (int)xlo_f;
