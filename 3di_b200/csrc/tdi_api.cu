@@ -308,6 +308,8 @@ DBatch batch_view(const tdi_batch *bt, int f0, int nf)
     v.ctl = a.ctl + F0;
     v.act = a.act + F0;
     v.nact = 0;
+    v.rlist = a.rlist + F0;
+    v.rcount = a.rcount + F0;
     v.geo = a.geo + F0 * m.V; v.proj = a.proj + F0 * m.V;
     v.zbuf = a.zbuf + F0 * NPIX;
     v.tri_mask = a.tri_mask + F0 * mask_words(m.T);
@@ -355,9 +357,11 @@ tdi_status compact_active(tdi_batch *bt, cudaStream_t s, int *n)
 
 tdi_status geometry(const Launch &L, const Cfg &c, int stage)
 {
-    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
+    // the pre-render checks need only the landmarks: a rejected trial skips the vertex stage
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
-                   (size_t)PC_WARPS * (2 * L.m.K + 4 * NL) * sizeof(float), L.s, L.m, L.b, c, stage));
+                   (size_t)PC_WARPS * (2 * L.m.K + 4 * NL + NL * PC_LM) * sizeof(float), L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, 0, k_compact_render, dim3(1), dim3(1024), 0, L.s, L.b));
+    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RESOLVE, k_raster_resolve, dim3(L.A()), dim3(RR_THREADS), 0, L.s, L.m, L.b));
     return TDI_OK;
@@ -616,7 +620,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
-    A(d.ctl, F); A(d.act, F); A(d.geo, F * (size_t)md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
+    A(d.ctl, F); A(d.act, F); A(d.rlist, F); A(d.rcount, F); A(d.geo, F * (size_t)md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
     A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
     A(d.J, F * NMAX * KTP); b->ne_frame_doubles = NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8);
     A(d.ne_part, F * b->ne_frame_doubles); A(d.err, 1); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 2);
@@ -938,6 +942,7 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     TDI_TRY(compact_active(b, s, &n));
     if (n > 0) {
         TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
+        TDI_TRY(launch(b, 0, k_compact_render, dim3(1), dim3(1024), 0, s, (const DBatch)d));
         TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, 8), L.smem_vertex(), s, m, d));
         TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, n), dim3(RD_THREADS), 0, s, m, d));
         TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));

@@ -115,6 +115,8 @@ struct DBatch {
     FrameCtl *ctl;           // [F]
     int32_t *act;            // [F] frames running the stage at the start of the round, ascending
     int32_t nact;            // entries of act
+    int32_t *rlist;          // [F] frames of act that render this round (after the pre-checks)
+    int32_t *rcount;         // [F]: rcount[0] = entries of rlist (one counter per view)
     // per-render working set
     float4 *geo;             // [F][V]: X0, Y0, Z0 and the albedo of the vertex (slot order)
     float4 *proj;            // [F][V]: xp, yp, camera Z, 0 -- what the raster gathers

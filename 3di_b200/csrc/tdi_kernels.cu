@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
     __syncthreads();
     if (tid < VT_F) {
         const int ai = f0 + tid;
-        const int f = ai < b.nact ? b.act[ai] : -1;
+        const int f = ai < b.rcount[0] ? b.rlist[ai] : -1;
         const int r = f >= 0 && b.ctl[f].render;
         s_frame[tid] = f;
         s_render[tid] = r;
@@ -331,17 +331,14 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
 // lane 0 sums them sequentially in FP64 in the oracle's order.
 
 __device__ __forceinline__ void landmark_G(const DModel &m, const DBatch &b, int f, const float *x,
-                                           const float *R, int i, float G[4])
+                                           const float *R, int i, const float *p, float G[4])
 {
     const float *tau = x + m.K;
-    const float4 *geo = b.geo + (size_t)f * m.V;
     const float *cam = b.cam + f * 4;
     const float fs = b.face_size[f];
     const float *bnd = b.bounds + (size_t)f * 4 * NL;
     const float xl = b.xl[f * NL + i], yl = b.yl[f * NL + i];
-    const int v = m.lis[i];
-    const float4 pv = geo[v];
-    const float p0 = pv.x, p1 = pv.y, p2 = pv.z;
+    const float p0 = p[0], p1 = p[1], p2 = p[2];
     const float r1p = (R[0] * p0 + R[3] * p1) + R[6] * p2;
     const float r2p = (R[1] * p0 + R[4] * p1) + R[7] * p2;
     const float r3p = (R[2] * p0 + R[5] * p1) + R[8] * p2;
@@ -355,32 +352,60 @@ __device__ __forceinline__ void landmark_G(const DModel &m, const DBatch &b, int
 
 // Face-size check (renderer.cu:838-857), barrier objective and the pre-render decisions of
 // a trial (model_fitter.cu:237-300): tau_z, face size, NaN barrier, then -g.d < 3e-4.
+// Both need only the 51 landmark vertices, so they run before the vertex stage: the landmark
+// object points and projections are formed here with the vertex stage's arithmetic (the same
+// values bit for bit), and a trial rejected here costs no vertex stage and no raster.
 constexpr int PC_WARPS = 4;
+constexpr int PC_LM = 5;                         // per landmark: X0, Y0, Z0, xp, yp
 
 __global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, Cfg c, int stage)
 {
-    extern __shared__ float pterm[];             // [PC_WARPS][2K + 4*NL]
+    extern __shared__ float pterm[];             // [PC_WARPS][2K + 4*NL], then [PC_WARPS][NL][PC_LM]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * PC_WARPS + warp;
     if (i >= b.nact) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active || !ctl.render) return;
-    const float4 *pj = b.proj + (size_t)f * m.V;
-    const int *L = m.lis;
-    const float d_iod = fabsf(pj[L[9]].x - pj[L[0]].x);
-    const float d_lem = fabsf(pj[L[0]].y - pj[L[40]].y);
-    const float d_rem = fabsf(pj[L[9]].y - pj[L[40]].y);
+    const int nterm = 2 * m.K + 4 * NL;
+    float *lm = pterm + PC_WARPS * nterm + warp * NL * PC_LM;
+    const float *x = b.xe + (size_t)f * m.KTP;
+    const float *R = b.R + f * 9;
+    {
+        const int K = m.K, KP = m.KP;
+        const float *tau = x + K;
+        const float *cam = b.cam + f * 4;
+        for (int li = lane; li < NL; li += 32) {
+            const int v = m.lis[li];
+            const float *er = m.E + (size_t)v * 3 * KP;
+            float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+            for (int k = 0; k < K; ++k) {
+                const float xk = x[k];
+                a0 = fmaf(er[k], xk, a0);
+                a1 = fmaf(er[KP + k], xk, a1);
+                a2 = fmaf(er[2 * KP + k], xk, a2);
+            }
+            const float X0 = m.mean[v] + a0, Y0 = m.mean[m.V + v] + a1, Z0 = m.mean[2 * m.V + v] + a2;
+            const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
+            const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
+            const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
+            float *o = lm + li * PC_LM;
+            o[0] = X0; o[1] = Y0; o[2] = Z0;
+            o[3] = (cam[0] * X3) / Z3 + cam[2];
+            o[4] = (cam[1] * Y3) / Z3 + cam[3];
+        }
+        __syncwarp();
+    }
+    const float d_iod = fabsf(lm[9 * PC_LM + 3] - lm[0 * PC_LM + 3]);
+    const float d_lem = fabsf(lm[0 * PC_LM + 4] - lm[40 * PC_LM + 4]);
+    const float d_rem = fabsf(lm[9 * PC_LM + 4] - lm[40 * PC_LM + 4]);
     const double lim = (double)c.ref_face_size * 2;
     const int face_ok = !((double)d_iod > lim || (double)d_lem > lim || (double)d_rem > lim);
     if (!shape_stage(stage)) {
         if (lane == 0) ctl.face_ok = face_ok;
         return;
     }
-    const int nterm = 2 * m.K + 4 * NL;
     float *t = pterm + warp * nterm;
-    const float *x = b.xe + (size_t)f * m.KTP;
-    const float *R = b.R + f * 9;
     const bool ft = stage == ST_FINETUNE;
     const float *lb = m.eps_b + (ft ? 2 : 0) * m.K;
     const float *ub = m.eps_b + (ft ? 3 : 1) * m.K;
@@ -392,7 +417,7 @@ __global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, 
     }
     for (int li = lane; li < NL; li += 32) {
         float G[4];
-        landmark_G(m, b, f, x, R, li, G);
+        landmark_G(m, b, f, x, R, li, lm + li * PC_LM, G);
         for (int sset = 0; sset < 4; ++sset) t[2 * m.K + sset * NL + li] = -(float)log((double)G[sset]);
     }
     __syncwarp();
@@ -1909,6 +1934,38 @@ __global__ void k_paint(DModel m, DBatch b, float *images, int32_t *tri_map)
         images[(size_t)f * NPIX + p] = s.tex;
         tri_map[(size_t)f * NPIX + p] = fr.tri;
     }
+}
+
+// Frames of the active list that render this round, in ascending order (one block).
+__global__ void __launch_bounds__(1024) k_compact_render(DBatch b)
+{
+    __shared__ int s_warp[32];
+    __shared__ int s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    for (int i0 = 0; i0 < b.nact; i0 += 1024) {
+        const int i = i0 + tid;
+        const int f = i < b.nact ? b.act[i] : -1;
+        const int r = f >= 0 && b.ctl[f].render;
+        const unsigned mask = __ballot_sync(0xffffffffu, r);
+        if (lane == 0) s_warp[warp] = __popc(mask);
+        __syncthreads();
+        if (tid < 32) {
+            int v = s_warp[tid], incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (tid >= o) incl += t;
+            }
+            s_warp[tid] = incl - v;
+        }
+        __syncthreads();
+        if (r) b.rlist[s_base + s_warp[warp] + __popc(mask & ((1u << lane) - 1u))] = f;
+        __syncthreads();
+        if (tid == 1023) s_base += s_warp[31] + __popc(mask);
+        __syncthreads();
+    }
+    if (tid == 0) b.rcount[0] = s_base;
 }
 
 // Frames still running the current stage, in ascending order (one block, block-wide scan).
