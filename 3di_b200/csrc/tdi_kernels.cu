@@ -1137,21 +1137,22 @@ __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
         atomicAdd(&cnt[p >> 1], (p & 1) ? 0x10000u : 1u);
     }
     __syncthreads();
-    // per-word distinct and extra counts, then an exclusive scan over the 2048 words
-    uint32_t u2[2], e2[2];
-    for (int q = 0; q < 2; ++q) {
-        const int w = tid * 2 + q;
-        uint32_t bb = 0, tb = 0, u = 0, e = 0;
-        for (int j = 0; j < 32; ++j) {
-            const uint32_t cv = cnt_at(cnt, w * 32 + j);
-            if (cv) { bb |= 1u << j; u++; }
-            if (cv > 1) { tb |= 1u << j; e += cv - 1; }
-        }
-        bits[w] = bb; tieb[w] = tb; u2[q] = u; e2[q] = e;
+    // per-word distinct and extra counts (a warp per word, a lane per pixel), then an
+    // exclusive scan over the 2048 words
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int w = warp; w < NPIX / 32; w += 32) {
+        const uint32_t cv = cnt_at(cnt, w * 32 + lane);
+        const uint32_t bb = __ballot_sync(0xffffffffu, cv != 0);
+        const uint32_t tb = __ballot_sync(0xffffffffu, cv > 1);
+        const uint32_t e = __reduce_add_sync(0xffffffffu, cv > 1 ? cv - 1 : 0u);
+        if (lane == 0) { bits[w] = bb; tieb[w] = tb; wU[w] = __popc(bb); wE[w] = e; }
     }
+    __syncthreads();
+    uint32_t u2[2], e2[2];
+    for (int q = 0; q < 2; ++q) { u2[q] = wU[tid * 2 + q]; e2[q] = wE[tid * 2 + q]; }
+    __syncthreads();                       // wU and wE are overwritten with the scan below
     uint32_t us = u2[0] + u2[1], es = e2[0] + e2[1];
     uint32_t ui = us, ei = es;   // inclusive warp scans
-    const int lane = tid & 31, warp = tid >> 5;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t a = __shfl_up_sync(0xffffffffu, ui, o), c2 = __shfl_up_sync(0xffffffffu, ei, o);
         if (lane >= o) { ui += a; ei += c2; }
