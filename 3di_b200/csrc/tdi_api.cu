@@ -241,7 +241,7 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_render, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   RENDER_SMEM_FLOATS * (int)sizeof(float)));
     TDI_CUDA(cudaFuncSetAttribute(k_neighbours, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t))));
+                                  (int)neigh_smem()));
     TDI_CUDA(cudaFuncSetAttribute(k_vertex, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_barrier_full, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -262,10 +262,11 @@ dim3 vertex_grid(const DModel &m, int frames)
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
     }
-    const int ftiles = (frames + VT_F - 1) / VT_F;
-    const int ntiles = (m.V + VT_V - 1) / VT_V;
-    const int groups = std::max(1, std::min(ntiles, VT_BLOCKS_PER_SM * sms / std::max(ftiles, 1)));
-    return dim3(std::max(ftiles, 1), groups);
+    // the kernel splits the blocks between frame tiles and vertex stripes by the number of
+    // frames that render, which is at most `frames`
+    const long ftiles = std::max(1, (frames + VT_F - 1) / VT_F);
+    const long ntiles = (m.V + VT_V - 1) / VT_V;
+    return dim3((unsigned)std::max(ftiles, std::min((long)VT_BLOCKS_PER_SM * sms, ftiles * ntiles)));
 }
 
 struct Launch {
@@ -275,7 +276,7 @@ struct Launch {
     cudaStream_t s;
     int F;
     size_t smem_vertex() const { return vt_smem(m.KP); }
-    size_t smem_neigh() const { return (NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t); }
+    size_t smem_neigh() const { return neigh_smem(); }
     size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * NE_P8 * sizeof(float); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
     size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
@@ -317,7 +318,6 @@ DBatch batch_view(const tdi_batch *bt, int f0, int nf)
     v.frag = a.frag + F0 * NMAX;
     v.fgrad = a.fgrad + F0 * 5 * NMAX;
     v.nb = a.nb + F0 * 4 * NMAX;
-    v.perm = a.perm + F0 * NMAX;
     v.J = a.J + F0 * NMAX * KTP;
     v.ne_part = a.ne_part + F0 * bt->ne_frame_doubles;
     v.img = a.img + F0 * 2 * NPIX;
@@ -621,7 +621,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
     A(d.ctl, F); A(d.act, F); A(d.rlist, F); A(d.rcount, F); A(d.geo, F * (size_t)md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
-    A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.perm, F * NMAX);
+    A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX);
     A(d.J, F * NMAX * KTP); b->ne_frame_doubles = NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8);
     A(d.ne_part, F * b->ne_frame_doubles); A(d.err, 1); A(d.img, F * 2 * NPIX); A(b->scalars, F * 4); A(b->d_count, 2);
     A(d.prof_frames, 1);

@@ -126,7 +126,6 @@ struct DBatch {
     Fragment *frag;          // [F][NMAX]
     float *fgrad;            // [F][5][NMAX]: gx, gy, h, gxs_n, gys_n
     int32_t *nb;             // [F][4][NMAX]: kl, kr, ka, kb
-    int32_t *perm;           // [F][NMAX]: sorted position -> fragment
     float *J;                // [F][NMAX][KTP]
     double *ne_part;         // [F][NMAX/256][part stride] chunk partials of the normal equations
     float *img;              // [F][2][NPIX] blur scratch for frames too large for shared memory

@@ -175,6 +175,10 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 // double-buffered so that the next tile streams in while this one is computed. A thread
 // owns one vertex x 8 frames (24 FMA chains). geo[f][slot] = (X0, Y0, Z0, albedo);
 // proj[f][slot] = (xp, yp, camera Z, 0).
+// The grid is one-dimensional (about two blocks per SM) and is split on the device by the
+// number of frames that render this round (known only there): ftiles frame tiles x groups
+// vertex-tile stripes, so that every block has work whatever share of the active frames
+// the pre-render checks rejected.
 
 constexpr int VT_V = 32;                                   // vertices per tile (one per lane)
 constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
@@ -197,28 +201,34 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
     __shared__ int s_any;
     __shared__ int s_render[VT_F], s_frame[VT_F];
     __shared__ __align__(8) uint64_t s_bar[2];
-    const int f0 = blockIdx.x * VT_F;
+    const int ntiles = (m.V + VT_V - 1) / VT_V;
+    const int rc = b.rcount[0];
+    const int ftiles = (rc + VT_F - 1) / VT_F;
+    if (ftiles == 0) return;
+    const int groups = max(1, min(ntiles, (int)gridDim.x / ftiles));
+    if ((int)blockIdx.x >= ftiles * groups) return;
+    const int gy = blockIdx.x / ftiles;        // vertex-tile stripe
+    const int f0 = (blockIdx.x - gy * ftiles) * VT_F;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     if (tid == 0) s_any = 0;
     __syncthreads();
     if (tid < VT_F) {
         const int ai = f0 + tid;
-        const int f = ai < b.rcount[0] ? b.rlist[ai] : -1;
+        const int f = ai < rc ? b.rlist[ai] : -1;
         const int r = f >= 0 && b.ctl[f].render;
         s_frame[tid] = f;
         s_render[tid] = r;
         if (r) {
             s_any = 1;
-            if (blockIdx.y == 0) prof_count(b, KID_VERTEX);
+            if (gy == 0) prof_count(b, KID_VERTEX);
         }
     }
     __syncthreads();
     if (!s_any) return;
-    const int ntiles = (m.V + VT_V - 1) / VT_V;
     const int rowbytes = 3 * KP * (int)sizeof(float);
     const uint32_t eb_addr = smem_addr(Eb);
     auto issue = [&](int j) {                  // thread 0: tile j of this block into buffer j & 1
-        const int t = blockIdx.y + j * gridDim.y;
+        const int t = gy + j * groups;
         if (t >= ntiles) return;
         const int nv = min(VT_V, m.V - t * VT_V), buf = j & 1;
         const uint32_t bar = smem_addr(&s_bar[buf]);
@@ -251,7 +261,7 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
     int j = 0;
     bool ok = true;
     for (;; ++j) {
-        const int t = blockIdx.y + j * gridDim.y;
+        const int t = gy + j * groups;
         if (t >= ntiles) break;
         const int buf = j & 1;
         const bool w = mbar_wait(smem_addr(&s_bar[buf]), (uint32_t)((j >> 1) & 1));
@@ -316,7 +326,7 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
         if (tid == 0) {
             atomicOr(b.err, 2);
             mbar_wait(smem_addr(&s_bar[j & 1]), (uint32_t)((j >> 1) & 1));
-            if (blockIdx.y + (j + 1) * gridDim.y < ntiles)
+            if (gy + (j + 1) * groups < ntiles)
                 mbar_wait(smem_addr(&s_bar[(j + 1) & 1]), (uint32_t)(((j + 1) >> 1) & 1));
         }
         __syncthreads();
@@ -1105,6 +1115,18 @@ __global__ void k_decide_lambda(DModel m, DBatch b, Cfg c)
 // all 0, where cum counts distinct covered pixels up to a pixel. Here the sort is replaced by
 // a counting placement: sorted position = distinct pixels below p + extra (tied) fragments
 // below p + rank among the fragments of p in slot order.
+// The counting atomics also build the per-word masks (covered pixels, pixels with 2+
+// fragments) and extra-fragment counts, so only 2,048 words are scanned. Sorted positions
+// and the inverse permutation are held in shared memory as 16-bit indices (NMAX = 32768).
+// A pixel hit by several fragments (rare) first gets its fragments placed in arbitrary order
+// inside its group, then each of them counts the group members with a lower slot index,
+// which gives the stable order; frames without such pixels skip those passes.
+
+constexpr int NB_U = 4;                 // fragment pixels loaded per thread before use
+__host__ __device__ constexpr size_t neigh_smem()
+{
+    return (size_t)(NPIX / 2 + 4 * (NPIX / 32)) * sizeof(uint32_t) + (size_t)NMAX * sizeof(uint16_t);
+}
 
 __device__ __forceinline__ uint32_t cnt_at(const uint32_t *cnt, int p)
 {
@@ -1117,40 +1139,56 @@ __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
     FrameCtl &ctl = b.ctl[f];
     if (!(all_frames ? ctl.render : ctl.need_jac)) return;
     if (threadIdx.x == 0) prof_count(b, KID_NEIGHBOURS);
-    extern __shared__ uint32_t nsm[];
+    extern __shared__ __align__(16) uint32_t nsm[];
     uint32_t *cnt = nsm;                    // 32768 words: two 16-bit counts each
+    uint16_t *perm = reinterpret_cast<uint16_t *>(nsm);   // replaces cnt: sorted position -> fragment
     uint32_t *bits = cnt + NPIX / 2;        // 2048 words: covered pixels
     uint32_t *tieb = bits + NPIX / 32;      // 2048 words: pixels with 2+ fragments
     uint32_t *wU = tieb + NPIX / 32;        // 2048: distinct pixels before the word
-    uint32_t *wE = wU + NPIX / 32;          // 2048: extra fragments before the word
+    uint32_t *wE = wU + NPIX / 32;          // 2048: extra fragments in (then before) the word
+    uint16_t *spos = reinterpret_cast<uint16_t *>(wE + NPIX / 32);   // [NMAX]: fragment -> sorted position
     __shared__ uint32_t s_wsum[2][32];
     __shared__ uint32_t s_flags;
-    const int tid = threadIdx.x;
+    __shared__ int s_ties;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int N = ctl.N;
     const Fragment *frags = b.frag + (size_t)f * NMAX;
-    int32_t *perm = b.perm + (size_t)f * NMAX;   // sorted position -> fragment
-    if (tid == 0) s_flags = 0;
-    for (int i = tid; i < NPIX / 2; i += 1024) cnt[i] = 0;
-    __syncthreads();
-    for (int n = tid; n < N; n += 1024) {
-        const int p = frags[n].pix_owner & 0xFFFF;
-        atomicAdd(&cnt[p >> 1], (p & 1) ? 0x10000u : 1u);
+    auto pix_of = [&](int n) -> int { return (int)(frags[n].pix_owner & 0xFFFF); };
+    auto load_pix = [&](int n0, int pv[NB_U]) {
+#pragma unroll
+        for (int u = 0; u < NB_U; ++u) {
+            const int n = n0 + u * 1024;
+            pv[u] = n < N ? pix_of(n) : 0;
+        }
+    };
+    if (tid == 0) { s_flags = 0; s_ties = 0; }
+    {
+        uint4 *z = reinterpret_cast<uint4 *>(nsm);          // cnt, bits, tieb
+        for (int i = tid; i < (NPIX / 2 + 2 * (NPIX / 32)) / 4; i += 1024) z[i] = make_uint4(0u, 0u, 0u, 0u);
+        for (int i = tid; i < NPIX / 32; i += 1024) wE[i] = 0;
     }
     __syncthreads();
-    // per-word distinct and extra counts (a warp per word, a lane per pixel), then an
-    // exclusive scan over the 2048 words
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int w = warp; w < NPIX / 32; w += 32) {
-        const uint32_t cv = cnt_at(cnt, w * 32 + lane);
-        const uint32_t bb = __ballot_sync(0xffffffffu, cv != 0);
-        const uint32_t tb = __ballot_sync(0xffffffffu, cv > 1);
-        const uint32_t e = __reduce_add_sync(0xffffffffu, cv > 1 ? cv - 1 : 0u);
-        if (lane == 0) { bits[w] = bb; tieb[w] = tb; wU[w] = __popc(bb); wE[w] = e; }
+    for (int n0 = tid; n0 < N; n0 += 1024 * NB_U) {
+        int pv[NB_U];
+        load_pix(n0, pv);
+#pragma unroll
+        for (int u = 0; u < NB_U; ++u) {
+            if (n0 + u * 1024 >= N) break;
+            const int p = pv[u], w = p >> 5;
+            const uint32_t bm = 1u << (p & 31), sh = (p & 1) * 16;
+            const uint32_t old = (atomicAdd(&cnt[p >> 1], 1u << sh) >> sh) & 0xFFFFu;
+            if (old == 0) {
+                atomicOr(&bits[w], bm);
+            } else {
+                atomicAdd(&wE[w], 1u);
+                if (old == 1) { atomicOr(&tieb[w], bm); s_ties = 1; }
+            }
+        }
     }
     __syncthreads();
+    // exclusive scans of the distinct and extra counts over the 2048 words
     uint32_t u2[2], e2[2];
-    for (int q = 0; q < 2; ++q) { u2[q] = wU[tid * 2 + q]; e2[q] = wE[tid * 2 + q]; }
-    __syncthreads();                       // wU and wE are overwritten with the scan below
+    for (int q = 0; q < 2; ++q) { u2[q] = __popc(bits[tid * 2 + q]); e2[q] = wE[tid * 2 + q]; }
     uint32_t us = u2[0] + u2[1], es = e2[0] + e2[1];
     uint32_t ui = us, ei = es;   // inclusive warp scans
     for (int o = 1; o < 32; o <<= 1) {
@@ -1158,7 +1196,7 @@ __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
         if (lane >= o) { ui += a; ei += c2; }
     }
     if (lane == 31) { s_wsum[0][warp] = ui; s_wsum[1][warp] = ei; }
-    __syncthreads();
+    __syncthreads();                       // also orders every read of wE above before its rewrite
     if (tid < 32) {
         uint32_t a = s_wsum[0][tid], c2 = s_wsum[1][tid];
         uint32_t ai = a, ci = c2;
@@ -1176,55 +1214,103 @@ __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
         wU[tid * 2 + 1] = ubase + u2[0]; wE[tid * 2 + 1] = ebase + e2[0];
     }
     __syncthreads();
-    auto distinct_below = [&](int p) -> uint32_t {     // covered pixels q < p
-        const int w = p >> 5, bit = p & 31;
-        return wU[w] + __popc(bits[w] & ((1u << bit) - 1u));
-    };
+    const bool ties = s_ties != 0;
     auto cum = [&](int p) -> int {                     // covered pixels q <= p
         const int w = p >> 5, bit = p & 31;
         return (int)(wU[w] + __popc(bits[w] & ((2u << bit) - 1u)));
     };
-    auto sorted_pos = [&](int n) -> int {
-        const int p = frags[n].pix_owner & 0xFFFF;
-        const int w = p >> 5, bit = p & 31;
-        uint32_t pos = distinct_below(p) + wE[w];
-        uint32_t tb = tieb[w] & ((1u << bit) - 1u);
+    auto tied = [&](int p) -> bool { return (tieb[p >> 5] >> (p & 31)) & 1u; };
+    // first sorted position of pixel p's fragments
+    auto group_start = [&](int p) -> int {
+        const int w = p >> 5;
+        const uint32_t below = (1u << (p & 31)) - 1u;
+        uint32_t pos = wU[w] + __popc(bits[w] & below) + wE[w];
+        uint32_t tb = tieb[w] & below;
         while (tb) {
             const int j = __ffs(tb) - 1;
             tb &= tb - 1;
             pos += cnt_at(cnt, w * 32 + j) - 1;
         }
-        if (cnt_at(cnt, p) > 1) {
-            uint32_t r = 0;
-            for (int q = 0; q < n; ++q) r += ((frags[q].pix_owner & 0xFFFF) == (uint32_t)p);
-            pos += r;
-        }
         return (int)pos;
     };
-    for (int n = tid; n < N; n += 1024) perm[sorted_pos(n)] = n;
-    __syncthreads();
-    int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
-    for (int n = tid; n < N; n += 1024) {
-        const int i = sorted_pos(n);
-        int S[4] = {0, 0, 0, 0};
-        if (i != 0 && i != N - 1) {
-            const int p = frags[n].pix_owner & 0xFFFF;
-            const int y = p & 255, x = p >> 8;
-            const int right = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
-            const int left = (x > 0) ? (x - 1) * DIM + y : 0;
-            const int dl = cum(p) - cum(left);
-            int kl = (i > dl) ? (i - dl) : 0;
-            kl = (uint16_t)kl;
-            if (kl >= N - 1) kl = N - 1;
-            S[0] = kl;
-            S[1] = (uint16_t)(i + cum(right) - cum(p));
-            S[2] = (uint16_t)(i - 1);
-            S[3] = (uint16_t)(i + 1);
+    for (int n0 = tid; n0 < N; n0 += 1024 * NB_U) {
+        int pv[NB_U];
+        load_pix(n0, pv);
+#pragma unroll
+        for (int u = 0; u < NB_U; ++u) {
+            const int n = n0 + u * 1024;
+            if (n < N) spos[n] = (uint16_t)group_start(pv[u]);
         }
-        for (int q = 0; q < 4; ++q) {
-            int sq = S[q];
-            if (sq >= N) { atomicOr(&s_flags, FLAG_OUT_OF_DOMAIN); sq = 0; }
-            nb[q * NMAX + n] = perm[sq];
+    }
+    if (ties) {
+        // distinct slots inside each group, in arbitrary order: the counts are taken back one
+        // by one (nothing reads them after the barrier)
+        __syncthreads();
+        for (int n = tid; n < N; n += 1024) {
+            const int p = pix_of(n);
+            if (!tied(p)) continue;
+            const uint32_t sh = (p & 1) * 16;
+            const uint32_t old = (atomicSub(&cnt[p >> 1], 1u << sh) >> sh) & 0xFFFFu;
+            spos[n] = (uint16_t)(spos[n] + old - 1);
+        }
+    }
+    __syncthreads();                       // the counts are no longer read: perm replaces them
+    for (int n = tid; n < N; n += 1024) perm[spos[n]] = (uint16_t)n;
+    __syncthreads();
+    if (ties) {
+        // stable order inside each group: rank = group members with a lower slot index
+        for (int n = tid; n < N; n += 1024) {
+            const int p = pix_of(n);
+            if (!tied(p)) continue;
+            const int i = spos[n];
+            int r = 0, j = i - 1;
+            for (; j >= 0; --j) {
+                const int q = perm[j];
+                if (pix_of(q) != p) break;
+                r += q < n;
+            }
+            const int start = j + 1;
+            for (j = i + 1; j < N; ++j) {
+                const int q = perm[j];
+                if (pix_of(q) != p) break;
+                r += q < n;
+            }
+            spos[n] = (uint16_t)(start + r);
+        }
+        __syncthreads();
+        for (int n = tid; n < N; n += 1024)
+            if (tied(pix_of(n))) perm[spos[n]] = (uint16_t)n;
+        __syncthreads();
+    }
+    int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
+    for (int n0 = tid; n0 < N; n0 += 1024 * NB_U) {
+        int pv[NB_U];
+        load_pix(n0, pv);
+#pragma unroll
+        for (int u = 0; u < NB_U; ++u) {
+            const int n = n0 + u * 1024;
+            if (n >= N) continue;
+            const int i = spos[n], p = pv[u];
+            int S[4] = {0, 0, 0, 0};
+            if (i != 0 && i != N - 1) {
+                const int y = p & 255, x = p >> 8;
+                const int right = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
+                const int left = (x > 0) ? (x - 1) * DIM + y : 0;
+                const int dl = cum(p) - cum(left);
+                int kl = (i > dl) ? (i - dl) : 0;
+                kl = (uint16_t)kl;
+                if (kl >= N - 1) kl = N - 1;
+                S[0] = kl;
+                S[1] = (uint16_t)(i + cum(right) - cum(p));
+                S[2] = (uint16_t)(i - 1);
+                S[3] = (uint16_t)(i + 1);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                int sq = S[q];
+                if (sq >= N) { atomicOr(&s_flags, FLAG_OUT_OF_DOMAIN); sq = 0; }
+                nb[q * NMAX + n] = perm[sq];
+            }
         }
     }
     __syncthreads();
