@@ -376,7 +376,7 @@ tdi_status render(const Launch &L, const Cfg &c, int stage)
 tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
 {
     TDI_TRY(launch(L.bt, KID_NEIGHBOURS, k_neighbours, dim3(L.A()), dim3(1024), L.smem_neigh(), L.s, L.b, 0));
-    TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(32, L.A()), dim3(JAC_WARPS * 32), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_JACOBIAN, k_jacobian, dim3(JAC_BPF, L.A()), dim3(JAC_THREADS), 0, L.s, L.m, L.b));
     if (c.normal_eq == 1) {
         // column groups of 8 per thread: 11 cover the reference's 79 expressions and the
         // weight column

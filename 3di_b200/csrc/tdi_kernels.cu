@@ -1318,79 +1318,100 @@ __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
 }
 
 // ------------------------------------------------------------------------------------------
-// Jacobian rows dI/dtheta (newfuncs.cu:173-299, funcs.cu:224-282): one warp per fragment,
-// lanes over the expression components; pose columns after them.
+// Jacobian rows dI/dtheta (newfuncs.cu:173-299, funcs.cu:224-282). A block takes chunks of
+// JAC_CH fragments of one frame: one thread per fragment forms the interpolated point, its
+// camera coordinates and the pose columns, and leaves the per-fragment factors in shared
+// memory; then the chunk's (fragment, expression column) items are spread over all threads,
+// consecutive items being consecutive columns of a fragment, so that the three basis rows
+// are read coalesced and no lane idles on a short last pass.
 
-constexpr int JAC_WARPS = 8;
+constexpr int JAC_THREADS = 256;
+constexpr int JAC_CH = 128;                  // fragments per chunk
+constexpr int JAC_BPF = 32;                  // blocks per frame
 
-__global__ void __launch_bounds__(JAC_WARPS * 32) k_jacobian(DModel m, DBatch b)
+__global__ void __launch_bounds__(JAC_THREADS, 4) k_jacobian(DModel m, DBatch b)
 {
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_JACOBIAN);
-    const int N = ctl.N, K = m.K, KP = m.KP, V = m.V;
-    const int lane = threadIdx.x & 31;
+    __shared__ float4 s_w[JAC_CH];           // al, be, ga, gx
+    __shared__ float4 s_v[JAC_CH];           // vx, vy, vz, gy
+    __shared__ float2 s_c[JAC_CH];           // phix / vz^2, phiy / vz^2
+    __shared__ int4 s_e[JAC_CH];             // basis row offsets of b, c, a; Jacobian row offset
+    const int N = ctl.N, K = m.K, KP = m.KP, V = m.V, KTP = m.KTP;
+    const int tid = threadIdx.x;
     const float4 *geo = b.geo + (size_t)f * V;
-    const float *R = b.R + f * 9, *dR = b.dR + f * 27;
-    const float *tau = b.xe + (size_t)f * m.KTP + K;
+    const float *Rg = b.R + f * 9, *dR = b.dR + f * 27;
+    const float *tau = b.xe + (size_t)f * KTP + K;
     const float phix = b.cam[f * 4], phiy = b.cam[f * 4 + 1];
     const Fragment *frags = b.frag + (size_t)f * NMAX;
     const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
-    const int wstride = gridDim.x * JAC_WARPS;
-    for (int n = blockIdx.x * JAC_WARPS + (threadIdx.x >> 5); n < N; n += wstride) {
-        const Fragment fr = frags[n];
-        const int tri = fr.tri;
-        const int4 tc = __ldg(m.tl4 + tri);
-        const int ib = tc.x, ic = tc.y, ia = tc.z;
-        const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
-        const float4 gb = geo[ib], gc = geo[ic], ga4 = geo[ia];
-        const float b0x = gb.x, b0y = gb.y, b0z = gb.z;
-        const float c0x = gc.x, c0y = gc.y, c0z = gc.z;
-        const float a0x = ga4.x, a0y = ga4.y, a0z = ga4.z;
-        const float px = (b0x * al + c0x * be) + a0x * ga;
-        const float py = (b0y * al + c0y * be) + a0y * ga;
-        const float pz = (b0z * al + c0z * be) + a0z * ga;
-        float bX, bY, bZ, cX, cY, cZ, aX, aY, aZ;
-        camera_coords(R, tau, b0x, b0y, b0z, bX, bY, bZ);
-        camera_coords(R, tau, c0x, c0y, c0z, cX, cY, cZ);
-        camera_coords(R, tau, a0x, a0y, a0z, aX, aY, aZ);
-        const float vx = (bX * al + cX * be) + aX * ga;
-        const float vy = (bY * al + cY * be) + aY * ga;
-        const float vz = (bZ * al + cZ * be) + aZ * ga;
-        const float ivz = 1.0f / vz, ivz2 = ivz * ivz;
-        const float gx = fg[n], gy = fg[NMAX + n];
-        float *row = b.J + ((size_t)f * NMAX + n) * m.KTP;
-        const float *eb = m.E + (size_t)ib * 3 * KP, *ec = m.E + (size_t)ic * 3 * KP, *ea = m.E + (size_t)ia * 3 * KP;
-        for (int k = lane; k < K; k += 32) {
-            const float tx = (eb[k] * al + ec[k] * be) + ea[k] * ga;
-            const float ty = (eb[KP + k] * al + ec[KP + k] * be) + ea[KP + k] * ga;
-            const float tz = (eb[2 * KP + k] * al + ec[2 * KP + k] * be) + ea[2 * KP + k] * ga;
-            const float REX = (tx * R[0] + ty * R[3]) + tz * R[6];
-            const float REY = (tx * R[1] + ty * R[4]) + tz * R[7];
-            const float REZ = (tx * R[2] + ty * R[5]) + tz * R[8];
-            const float nwx = (phix * ivz2) * (REX * vz - REZ * vx);
-            const float nwy = (phiy * ivz2) * (REY * vz - REZ * vy);
-            row[k] = -(gx * nwx + gy * nwy);
-        }
-        if (lane < 6) {
-            float val;
-            if (lane == 0) val = -(gx * (phix * ivz) + gy * 0.0f);
-            else if (lane == 1) val = -(gx * 0.0f + gy * (phiy * ivz));
-            else if (lane == 2) val = -(gx * (((-phix) * vx) * ivz2) + gy * (((-phiy) * vy) * ivz2));
-            else {
-                const float *d = dR + 9 * (lane - 3);
+    float *Jf = b.J + (size_t)f * NMAX * KTP;
+    float R[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) R[i] = Rg[i];
+    const uint32_t mg = 0xFFFFFFFFu / (uint32_t)K + 1u;   // i / K = umulhi(i, mg) for i < 2^16
+    for (int c0 = blockIdx.x * JAC_CH; c0 < N; c0 += gridDim.x * JAC_CH) {
+        const int cnt = min(JAC_CH, N - c0);
+        if (tid < cnt) {
+            const int n = c0 + tid;
+            const Fragment fr = frags[n];
+            const int4 tc = __ldg(m.tl4 + fr.tri);
+            const int ib = tc.x, ic = tc.y, ia = tc.z;
+            const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
+            const float4 gb = geo[ib], gc = geo[ic], ga4 = geo[ia];
+            const float px = (gb.x * al + gc.x * be) + ga4.x * ga;
+            const float py = (gb.y * al + gc.y * be) + ga4.y * ga;
+            const float pz = (gb.z * al + gc.z * be) + ga4.z * ga;
+            float bX, bY, bZ, cX, cY, cZ, aX, aY, aZ;
+            camera_coords(R, tau, gb.x, gb.y, gb.z, bX, bY, bZ);
+            camera_coords(R, tau, gc.x, gc.y, gc.z, cX, cY, cZ);
+            camera_coords(R, tau, ga4.x, ga4.y, ga4.z, aX, aY, aZ);
+            const float vx = (bX * al + cX * be) + aX * ga;
+            const float vy = (bY * al + cY * be) + aY * ga;
+            const float vz = (bZ * al + cZ * be) + aZ * ga;
+            const float ivz = 1.0f / vz, ivz2 = ivz * ivz;
+            const float gx = fg[n], gy = fg[NMAX + n];
+            s_w[tid] = make_float4(al, be, ga, gx);
+            s_v[tid] = make_float4(vx, vy, vz, gy);
+            s_c[tid] = make_float2(phix * ivz2, phiy * ivz2);
+            s_e[tid] = make_int4(ib * 3 * KP, ic * 3 * KP, ia * 3 * KP, n * KTP);
+            float *row = Jf + (size_t)n * KTP;
+            row[K + 0] = -(gx * (phix * ivz) + gy * 0.0f);
+            row[K + 1] = -(gx * 0.0f + gy * (phiy * ivz));
+            row[K + 2] = -(gx * (((-phix) * vx) * ivz2) + gy * (((-phiy) * vy) * ivz2));
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float *d = dR + 9 * j;
                 const float dvx = (d[0] * px + d[3] * py) + d[6] * pz;
                 const float dvy = (d[1] * px + d[4] * py) + d[7] * pz;
                 const float dvz = (d[2] * px + d[5] * py) + d[8] * pz;
                 const float dWx = (phix * ivz2) * (vz * dvx - vx * dvz);
                 const float dWy = (phiy * ivz2) * (vz * dvy - vy * dvz);
-                val = -(gx * dWx + gy * dWy);
+                row[K + 3 + j] = -(gx * dWx + gy * dWy);
             }
-            row[K + lane] = val;
-        } else if (lane < 6 + (m.KTP - m.KT)) {
-            row[m.KT + lane - 6] = 0.0f;
+            for (int j = m.KT; j < KTP; ++j) row[j] = 0.0f;
         }
+        __syncthreads();
+#pragma unroll 2
+        for (int i = tid; i < cnt * K; i += JAC_THREADS) {
+            const int nl = (int)__umulhi((uint32_t)i, mg), k = i - nl * K;
+            const float4 w = s_w[nl], v = s_v[nl];
+            const float2 cc = s_c[nl];
+            const int4 e = s_e[nl];
+            const float *eb = m.E + e.x + k, *ec = m.E + e.y + k, *ea = m.E + e.z + k;
+            const float tx = (__ldg(eb) * w.x + __ldg(ec) * w.y) + __ldg(ea) * w.z;
+            const float ty = (__ldg(eb + KP) * w.x + __ldg(ec + KP) * w.y) + __ldg(ea + KP) * w.z;
+            const float tz = (__ldg(eb + 2 * KP) * w.x + __ldg(ec + 2 * KP) * w.y) + __ldg(ea + 2 * KP) * w.z;
+            const float REX = (tx * R[0] + ty * R[3]) + tz * R[6];
+            const float REY = (tx * R[1] + ty * R[4]) + tz * R[7];
+            const float REZ = (tx * R[2] + ty * R[5]) + tz * R[8];
+            const float nwx = cc.x * (REX * v.z - REZ * v.x);
+            const float nwy = cc.y * (REY * v.z - REZ * v.y);
+            Jf[e.w + k] = -(w.w * nwx + v.w * nwy);
+        }
+        __syncthreads();
     }
 }
 
