@@ -900,64 +900,59 @@ __device__ __forceinline__ Shading shade(const DModel &m, const float4 *geo, con
     return s;
 }
 
-__device__ __forceinline__ void pixel_grad(const float *im, int x, int y, int rx0, int ry0, int rh,
-                                           float &gx, float &gy, float &h, float &gxn, float &gyn)
+// Normalised central-difference gradient of one pixel from its four neighbours as
+// fill_grads forms them (index 0 past the crop border): r, l = x + 1, x - 1; d, u = y + 1, y - 1.
+__device__ __forceinline__ void grad_of(float r, float l, float d, float u, float &gx, float &gy,
+                                        float &h, float &gxn, float &gyn)
 {
-    // neighbours as fill_grads forms them (index 0 past the crop border); the region holds
-    // every pixel these can name (the whole crop when the fragments touch its border)
-    const int kr = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
-    const int kl = (x > 0) ? (x - 1) * DIM + y : 0;
-    const int ka = (y > 0) ? x * DIM + y - 1 : 0;
-    const int kb = (y < DIM - 1) ? x * DIM + y + 1 : 0;
-    auto at = [&](int p) { return im[((p >> 8) - rx0) * rh + ((p & 255) - ry0)]; };
-    const float a = 0.5f * (at(kr) - at(kl));
-    const float bb = 0.5f * (at(kb) - at(ka));
+    const float a = 0.5f * (r - l);
+    const float bb = 0.5f * (d - u);
     const float hh = 1e-16f + sqrtf((4 * a) * a + (4 * bb) * bb);
     gx = a; gy = bb; h = hh;
     gxn = (2.0f * a) / hh;
     gyn = (2.0f * bb) / hh;
 }
 
-__device__ __forceinline__ void target_grad(const float *im, int ks, float &gxn, float &gyn)
+__device__ __forceinline__ void neighbour_pixels(int p, int &kr, int &kl, int &kd, int &ku)
 {
-    const int y = ks & 255, x = ks >> 8;
-    const int kr = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
-    const int kl = (x > 0) ? (x - 1) * DIM + y : 0;
-    const int ka = (y > 0) ? x * DIM + y - 1 : 0;
-    const int kb = (y < DIM - 1) ? x * DIM + y + 1 : 0;
-    const float a = 0.5f * (im[kr] - im[kl]);
-    const float bb = 0.5f * (im[kb] - im[ka]);
-    const float hh = 1e-16f + sqrtf((4 * a) * a + (4 * bb) * bb);
-    gxn = (2.0f * a) / hh;
-    gyn = (2.0f * bb) / hh;
+    const int y = p & 255, x = p >> 8;
+    kr = (x < DIM - 1) ? (x + 1) * DIM + y : 0;
+    kl = (x > 0) ? (x - 1) * DIM + y : 0;
+    ku = (y > 0) ? x * DIM + y - 1 : 0;
+    kd = (y < DIM - 1) ? x * DIM + y + 1 : 0;
 }
 
-constexpr int RENDER_THREADS = 256;
-constexpr int RENDER_SMEM_FLOATS = 16 * 1024;   // two region buffers of up to 8,192 pixels
-constexpr int RENDER_UNROLL = 4;                 // fragments whose gathers are in flight together
+// Region of the render: the fragment box + 8 px, or the whole crop when the fragments touch
+// its border (a border pixel's neighbour is pixel 0). Blur taps are summed in ascending
+// offset order with zeros outside the region (rows along y, then columns along x).
+// The region buffers carry KRAD zero lines on the blurred side, so the taps need no bounds
+// test: A[xl][KRAD + yl] (pitch rh + 2 KRAD) holds the shaded image and later the blurred
+// one, B[KRAD + xl][yl] (pitch rh) the row pass. They live in shared memory when they fit,
+// else in the frame's global buffer. Fragment gathers are issued RENDER_U at a time before
+// their results are stored.
 
-__global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, Cfg c, int stage)
+constexpr int RENDER_THREADS = 512;
+constexpr int RENDER_SMEM_FLOATS = 27 * 1024;     // padded region buffers (108 KB): two blocks per SM
+constexpr int RENDER_U = 2;                       // fragments whose gathers are in flight together
+constexpr int RENDER_GU = 2;                      // the same in the gradient pass (8 loads each)
+constexpr int RIMG = 2 * DIM * (DIM + 2 * KRAD);  // per-frame floats of the global fallback
+
+__host__ __device__ __forceinline__ int region_floats(int rw, int rh)
 {
-    const int f = b.act[blockIdx.x];
-    FrameCtl &ctl = b.ctl[f];
-    if (!ctl.render) return;
-    if (threadIdx.x == 0) prof_count(b, KID_RENDER);
-    extern __shared__ float rsm[];
-    __shared__ double s_red[RENDER_THREADS / 32];
+    return rw * (rh + 2 * KRAD) + (rw + 2 * KRAD) * rh;
+}
+
+template <bool SMEM>
+__device__ __forceinline__ void render_region(const DModel &m, const DBatch &b, const Cfg &c, int stage,
+                                              int f, FrameCtl &ctl, float *A, float *B, int rx0,
+                                              int ry0, int rw, int rh, double *s_red)
+{
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = RENDER_THREADS / 32;
     const int N = ctl.N;
-    const bool border = ctl.bbox[0] < 1 || ctl.bbox[1] > DIM - 2 || ctl.bbox[2] < 1 || ctl.bbox[3] > DIM - 2;
-    const int rx0 = border ? 0 : max(0, ctl.bbox[0] - 8), rx1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[1] + 8);
-    const int ry0 = border ? 0 : max(0, ctl.bbox[2] - 8), ry1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[3] + 8);
-    const int rw = rx1 - rx0 + 1, rh = ry1 - ry0 + 1;
-    const int area = rw * rh;
-    // the region (fragment box + 8 px) in shared memory, or in the frame's global buffer when
-    // it is larger than 8,192 pixels
-    float *A, *B;
-    if (2 * area <= RENDER_SMEM_FLOATS) { A = rsm; B = rsm + area; }
-    else { A = b.img + (size_t)f * 2 * NPIX; B = A + NPIX; }
-    for (int i = tid; i < area; i += RENDER_THREADS) A[i] = 0.0f;
+    const int ph = rh + 2 * KRAD;
+    for (int i = tid; i < rw * ph; i += RENDER_THREADS) A[i] = 0.0f;
+    for (int i = tid; i < KRAD * rh; i += RENDER_THREADS) { B[i] = 0.0f; B[(KRAD + rw) * rh + i] = 0.0f; }
     __syncthreads();
     const float4 *geo = b.geo + (size_t)f * m.V;
     const float *R = b.R + f * 9;
@@ -966,61 +961,84 @@ __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, C
     const float *lam = (stage == ST_LAMBDA && ctl.mode == M_TRIAL) ? b.lam_ls + f * 4 : b.lam + f * 4;
     const float Lint = b.Lint[f];
     const Fragment *frags = b.frag + (size_t)f * NMAX;
-    for (int n0 = tid; n0 < N; n0 += RENDER_THREADS * RENDER_UNROLL) {
-        Fragment fr[RENDER_UNROLL];
+    auto at = [&](int p) { return ((p >> 8) - rx0) * ph + KRAD + ((p & 255) - ry0); };
+    for (int n0 = tid; n0 < N; n0 += RENDER_THREADS * RENDER_U) {
+        Fragment fr[RENDER_U];
 #pragma unroll
-        for (int u = 0; u < RENDER_UNROLL; ++u) {
+        for (int u = 0; u < RENDER_U; ++u) {
             const int n = n0 + u * RENDER_THREADS;
             fr[u] = n < N ? frags[n] : Fragment{0u, 0, 0.0f, 0.0f};
         }
+        float tex[RENDER_U];
+        int idx[RENDER_U];
 #pragma unroll
-        for (int u = 0; u < RENDER_UNROLL; ++u) {
+        for (int u = 0; u < RENDER_U; ++u) {
+            idx[u] = -1;
+            tex[u] = 0.0f;
             if (fr[u].pix_owner & 0x80000000u) {
-                const Shading sh = shade(m, geo, fr[u], R, tau, lam, Lint);
-                const int p = fr[u].pix_owner & 0xFFFF;
-                A[((p >> 8) - rx0) * rh + ((p & 255) - ry0)] = sh.tex;
+                tex[u] = shade(m, geo, fr[u], R, tau, lam, Lint).tex;
+                idx[u] = at(fr[u].pix_owner & 0xFFFF);
             }
         }
+#pragma unroll
+        for (int u = 0; u < RENDER_U; ++u)
+            if (idx[u] >= 0) A[idx[u]] = tex[u];
     }
     __syncthreads();
-    // rows: along the contiguous (y) index; warps take columns, lanes take rows
-    for (int xl = warp; xl < rw; xl += NW)
-        for (int yl = lane; yl < rh; yl += 32) {
-            float s = 0.0f;
+    const uint32_t mgh = 0xFFFFFFFFu / (uint32_t)rh + 1u;   // i / rh = umulhi(i, mgh) for i <= 2^16
+    // rows: along the contiguous (y) index
+    for (int i = tid; i < rw * rh; i += RENDER_THREADS) {
+        const int xl = (int)__umulhi((uint32_t)i, mgh), yl = i - xl * rh;
+        const float *a = A + xl * ph + yl;               // a[KRAD + j] = A(xl, yl + j)
+        float s = 0.0f;
 #pragma unroll
-            for (int j = -KRAD; j <= KRAD; ++j) {
-                const int yy = yl + j;
-                const float v = (yy >= 0 && yy < rh) ? A[xl * rh + yy] : 0.0f;
-                s = s + c.taps[KRAD - j] * v;
-            }
-            B[xl * rh + yl] = s;
-        }
+        for (int j = -KRAD; j <= KRAD; ++j) s = s + c.taps[KRAD - j] * a[KRAD + j];
+        B[(KRAD + xl) * rh + yl] = s;
+    }
     __syncthreads();
     // columns: along the strided (x) index
-    for (int xl = warp; xl < rw; xl += NW)
-        for (int yl = lane; yl < rh; yl += 32) {
-            float s = 0.0f;
+    for (int i = tid; i < rw * rh; i += RENDER_THREADS) {
+        const int xl = (int)__umulhi((uint32_t)i, mgh), yl = i - xl * rh;
+        const float *bp = B + xl * rh + yl;              // bp[(KRAD + j) * rh] = B(xl + j, yl)
+        float s = 0.0f;
 #pragma unroll
-            for (int j = -KRAD; j <= KRAD; ++j) {
-                const int xx = xl + j;
-                const float v = (xx >= 0 && xx < rw) ? B[xx * rh + yl] : 0.0f;
-                s = s + c.taps[KRAD - j] * v;
-            }
-            A[xl * rh + yl] = s;
-        }
+        for (int j = -KRAD; j <= KRAD; ++j) s = s + c.taps[KRAD - j] * bp[(KRAD + j) * rh];
+        A[xl * ph + KRAD + yl] = s;
+    }
     __syncthreads();
     const float *tgt = b.target + (size_t)f * NPIX;
     float *fg = b.fgrad + (size_t)f * 5 * NMAX;
     double corr = 0.0;
-    for (int n = tid; n < N; n += RENDER_THREADS) {
-        const int p = frags[n].pix_owner & 0xFFFF;
-        const int x = p >> 8, y = p & 255;
-        float gx, gy, h, gxn, gyn, sxn, syn;
-        pixel_grad(A, x, y, rx0, ry0, rh, gx, gy, h, gxn, gyn);
-        target_grad(tgt, p, sxn, syn);
-        fg[n] = gx; fg[NMAX + n] = gy; fg[2 * NMAX + n] = h;
-        fg[3 * NMAX + n] = sxn; fg[4 * NMAX + n] = syn;
-        corr += (double)gxn * (double)sxn + (double)gyn * (double)syn;
+    for (int n0 = tid; n0 < N; n0 += RENDER_THREADS * RENDER_GU) {
+        int pv[RENDER_GU];
+#pragma unroll
+        for (int u = 0; u < RENDER_GU; ++u) {
+            const int n = n0 + u * RENDER_THREADS;
+            pv[u] = n < N ? (int)(frags[n].pix_owner & 0xFFFF) : -1;
+        }
+        float rv[RENDER_GU][4], tv[RENDER_GU][4];
+#pragma unroll
+        for (int u = 0; u < RENDER_GU; ++u) {
+            rv[u][0] = rv[u][1] = rv[u][2] = rv[u][3] = 0.0f;
+            tv[u][0] = tv[u][1] = tv[u][2] = tv[u][3] = 0.0f;
+            if (pv[u] >= 0) {                  // (pixel 0 lies outside a region that is not the crop)
+                int kr, kl, kd, ku;
+                neighbour_pixels(pv[u], kr, kl, kd, ku);
+                rv[u][0] = A[at(kr)]; rv[u][1] = A[at(kl)]; rv[u][2] = A[at(kd)]; rv[u][3] = A[at(ku)];
+                tv[u][0] = tgt[kr]; tv[u][1] = tgt[kl]; tv[u][2] = tgt[kd]; tv[u][3] = tgt[ku];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RENDER_GU; ++u) {
+            if (pv[u] < 0) break;
+            const int n = n0 + u * RENDER_THREADS;
+            float gx, gy, h, gxn, gyn, sx, sy, sh, sxn, syn;
+            grad_of(rv[u][0], rv[u][1], rv[u][2], rv[u][3], gx, gy, h, gxn, gyn);
+            grad_of(tv[u][0], tv[u][1], tv[u][2], tv[u][3], sx, sy, sh, sxn, syn);
+            fg[n] = gx; fg[NMAX + n] = gy; fg[2 * NMAX + n] = h;
+            fg[3 * NMAX + n] = sxn; fg[4 * NMAX + n] = syn;
+            corr += (double)gxn * (double)sxn + (double)gyn * (double)syn;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) corr += __shfl_down_sync(0xffffffffu, corr, o);
     if (lane == 0) s_red[warp] = corr;
@@ -1029,6 +1047,26 @@ __global__ void __launch_bounds__(RENDER_THREADS) k_render(DModel m, DBatch b, C
         double s = 0.0;
         for (int w = 0; w < NW; ++w) s += s_red[w];
         ctl.corr = s;
+    }
+}
+
+__global__ void __launch_bounds__(RENDER_THREADS, 2) k_render(DModel m, DBatch b, Cfg c, int stage)
+{
+    const int f = b.act[blockIdx.x];
+    FrameCtl &ctl = b.ctl[f];
+    if (!ctl.render) return;
+    if (threadIdx.x == 0) prof_count(b, KID_RENDER);
+    extern __shared__ __align__(16) float rsm[];
+    __shared__ double s_red[RENDER_THREADS / 32];
+    const bool border = ctl.bbox[0] < 1 || ctl.bbox[1] > DIM - 2 || ctl.bbox[2] < 1 || ctl.bbox[3] > DIM - 2;
+    const int rx0 = border ? 0 : max(0, ctl.bbox[0] - 8), rx1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[1] + 8);
+    const int ry0 = border ? 0 : max(0, ctl.bbox[2] - 8), ry1 = border ? DIM - 1 : min(DIM - 1, ctl.bbox[3] + 8);
+    const int rw = rx1 - rx0 + 1, rh = ry1 - ry0 + 1;
+    if (region_floats(rw, rh) <= RENDER_SMEM_FLOATS) {
+        render_region<true>(m, b, c, stage, f, ctl, rsm, rsm + rw * (rh + 2 * KRAD), rx0, ry0, rw, rh, s_red);
+    } else {
+        float *g = b.img + (size_t)f * RIMG;
+        render_region<false>(m, b, c, stage, f, ctl, g, g + rw * (rh + 2 * KRAD), rx0, ry0, rw, rh, s_red);
     }
 }
 
