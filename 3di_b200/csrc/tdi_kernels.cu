@@ -1590,13 +1590,49 @@ __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, doubl
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
+// Rows are staged in shared memory as doubles (converted once when built), row pitch NE_PD:
+// 92 doubles puts the four rows a warp reads at once on disjoint bank groups.
+constexpr int NE_PD = NE_P8 + 4;
+
+// Tile list in ne_tile8's order, as a compile-time table.
+struct NeTiles {
+    int bi[NE_NT8], bj[NE_NT8];
+};
+__host__ __device__ constexpr NeTiles make_ne_tiles()
+{
+    NeTiles t{};
+    int k = 0;
+    for (int i = 0; i < NE_T8; ++i)
+        for (int j = i; j < NE_T8; ++j) { t.bi[k] = i; t.bj[k] = j; ++k; }
+    return t;
+}
+
+// The tensor-core updates of warp W (tiles W, W + 8, ...) over the fragment pairs of one
+// stage: a lane loads its row's value in each of the 11 column blocks once per pair and
+// feeds every tile from those registers.
+template <int W>
+__device__ __forceinline__ void ne_pairs(double (&acc)[NE_TPW][2], const double *rows, int cn, int kr, int fr8)
+{
+    constexpr NeTiles TT = make_ne_tiles();
+    constexpr int NT = (NE_NT8 - W + 7) / 8;
+    for (int q = 0; q + 2 <= cn; q += 2) {
+        const double *rk = rows + (size_t)(2 * q + kr) * NE_PD + fr8;
+        double v[NE_T8];
+#pragma unroll
+        for (int c = 0; c < NE_T8; ++c) v[c] = rk[8 * c];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma_884(acc[j][0], acc[j][1], v[TT.bi[W + 8 * j]], v[TT.bj[W + 8 * j]]);
+    }
+}
+
+
 __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
 {
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) prof_count(b, KID_NORMAL_EQ);
-    extern __shared__ __align__(16) float nesf[];   // rows [2][2*NE_SUB][NE_P8], FP32
+    extern __shared__ __align__(16) double nesd[];  // rows [2][2*NE_SUB][NE_PD]
     const int KTP = m.KTP, KT = m.KT;
     __shared__ ChunkHead hd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1625,7 +1661,7 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
         chunk_head(hd, fg, nb, c0, cnt);
         __syncthreads();
         for (int it = 0; it < nsub; ++it) {
-            float *rows = nesf + (size_t)(it & 1) * 2 * NE_SUB * NE_P8;
+            double *rows = nesd + (size_t)(it & 1) * 2 * NE_SUB * NE_PD;
             {
                 float v[NE_GRP][4];
                 const int ql = q_me, q = it * NE_SUB + ql;
@@ -1641,34 +1677,34 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
                         if (a < KT) chain_value(v[g], pre, diffx, diffy, ox, oy);
                         else if (a == KT) { ox = (float)hd.w[2 * q]; oy = (float)hd.w[2 * q + 1]; }
                     }
-                    rows[(2 * ql) * NE_P8 + a] = ox;
-                    rows[(2 * ql + 1) * NE_P8 + a] = oy;
+                    rows[(2 * ql) * NE_PD + a] = (double)ox;
+                    rows[(2 * ql + 1) * NE_PD + a] = (double)oy;
                 }
             }
             __syncthreads();
             const int cn = min(NE_SUB, cnt - it * NE_SUB);
             // pairs of fragments on the tensor cores
-            for (int q = 0; q + 2 <= cn; q += 2) {
-                const float *rk = rows + (size_t)(2 * q + kr) * NE_P8;
-#pragma unroll
-                for (int j = 0; j < NE_TPW; ++j) {
-                    if (tbi[j] < 0) continue;
-                    const double av = (double)rk[8 * tbi[j] + fr8];
-                    const double bv = (double)rk[8 * tbj[j] + fr8];
-                    dmma_884(acc[j][0], acc[j][1], av, bv);
-                }
+            switch (warp) {
+            case 0: ne_pairs<0>(acc, rows, cn, kr, fr8); break;
+            case 1: ne_pairs<1>(acc, rows, cn, kr, fr8); break;
+            case 2: ne_pairs<2>(acc, rows, cn, kr, fr8); break;
+            case 3: ne_pairs<3>(acc, rows, cn, kr, fr8); break;
+            case 4: ne_pairs<4>(acc, rows, cn, kr, fr8); break;
+            case 5: ne_pairs<5>(acc, rows, cn, kr, fr8); break;
+            case 6: ne_pairs<6>(acc, rows, cn, kr, fr8); break;
+            default: ne_pairs<7>(acc, rows, cn, kr, fr8); break;
             }
             // an odd last fragment: this thread's two entries of each tile, same chain
             if (cn & 1) {
                 const int q = cn - 1;
-                const float *rx = rows + (size_t)(2 * q) * NE_P8, *ry = rx + NE_P8;
+                const double *rx = rows + (size_t)(2 * q) * NE_PD, *ry = rx + NE_PD;
 #pragma unroll
                 for (int j = 0; j < NE_TPW; ++j) {
                     if (tbi[j] < 0) continue;
                     const int r = 8 * tbi[j] + fr8, c = 8 * tbj[j] + 2 * kr;
 #pragma unroll
                     for (int i = 0; i < 2; ++i)
-                        acc[j][i] = fma((double)ry[r], (double)ry[c + i], fma((double)rx[r], (double)rx[c + i], acc[j][i]));
+                        acc[j][i] = fma(ry[r], ry[c + i], fma(rx[r], rx[c + i], acc[j][i]));
                 }
             }
         }
