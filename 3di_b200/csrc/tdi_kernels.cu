@@ -466,6 +466,19 @@ __global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, 
 // does. The epoch tag makes earlier renders' keys lose to this one's without clearing the
 // z-buffer; it is cleared once the tag range is used up.
 
+// True when alpha + beta, formed as fl(fl(na / denom) + fl(nb / denom)), is certainly above
+// 1 for na, nb of denom's (nonzero) sign, so the two divisions can be skipped. With u = 2^-24:
+// a finite s = fl(na + nb) beyond lim = fl(denom (1 + 16u)) gives (na + nb) / denom > 1 + 13u
+// exactly, and the rounded quotients and their rounded sum then still exceed 1. Cases the bound
+// cannot settle (and |denom| below 1e-30) return false and take the exact test.
+__device__ __forceinline__ bool sum_exceeds_one(float na, float nb, float denom, bool dpos)
+{
+    constexpr float GROW = 1.0f + 16.0f * 5.9604644775390625e-8f;
+    const float s = na + nb, lim = denom * GROW;
+    const bool beyond = dpos ? s > lim : s < lim;
+    return beyond && fabsf(denom) >= 1e-30f && fabsf(s) <= 3.4028234663852886e38f;
+}
+
 // Samples of one triangle with corners b, c, a (rows 0, 1, 2 of the triangle list) in the
 // reference's order: x-major over the integer points of the bounding box, at most NTMP.
 // emit(r, pix, alpha, beta) receives each, pix wrapped to 16 bits as the reference's
@@ -503,34 +516,51 @@ __device__ __forceinline__ int tri_samples(float bx, float by, float cx, float c
     const bool dpos = denom > 0.0f;
     int ridx = 0;
     // Boxes of at most 2 x 2 sample points (almost every triangle of a dense face mesh): the
-    // same points in the same x-major order, evaluated without loops; at most 4 fragments, so
-    // the NTMP cap cannot bind.
+    // same points with the same FP32 operations, evaluated without branches (the candidates'
+    // products are formed once and shared, which rounds exactly as per point). Points whose
+    // alpha + beta certainly exceeds 1 are dropped before the divisions; the rest take the
+    // exact test in x-major order. At most 4 fragments, so the NTMP cap cannot bind.
     if (xhi - xlo_f <= 2.0f && yhi - ylo_f <= 2.0f) {
         const int xi0 = (int)xlo_f, yi0 = (int)ylo_f;
+        const float xf1 = xlo_f + 1.0f, yf1 = ylo_f + 1.0f;
+        // (the reference stops at the first coordinate outside the box; xf1 < xhi implies
+        // xlo_f < xhi, so these select the same points)
+        const bool okx[2] = {xlo_f < xhi, xf1 < xhi}, oky[2] = {ylo_f < yhi, yf1 < yhi};
+        const float v2x[2] = {xlo_f - ax, xf1 - ax}, v2y[2] = {ylo_f - ay, yf1 - ay};
+        float p0x[2], p1x[2], p0y[2], p1y[2];
 #pragma unroll
-        for (int ix = 0; ix < 2; ++ix) {
-            const float xf = xlo_f + (float)ix;
-            if (!(xf < xhi)) break;
-            const float v2x = xf - ax;
+        for (int i = 0; i < 2; ++i) {
+            p0x[i] = v0x * v2x[i]; p1x[i] = v1x * v2x[i];
+            p0y[i] = v0y * v2y[i]; p1y[i] = v1y * v2y[i];
+        }
+        float na[4], nb[4];
+        uint32_t cand = 0;
+#pragma unroll
+        for (int ix = 0; ix < 2; ++ix)
 #pragma unroll
             for (int iy = 0; iy < 2; ++iy) {
-                const float yf = ylo_f + (float)iy;
-                if (!(yf < yhi)) break;
-                const float v2y = yf - ay;
-                const float d20 = v0x * v2x + v0y * v2y;
-                const float d21 = v1x * v2x + v1y * v2y;
-                const float na = d11 * d20 - d01 * d21;
-                const float nb = d00 * d21 - d01 * d20;
-                if ((dpos ? na > 0.0f : na < 0.0f) && (dpos ? nb > 0.0f : nb < 0.0f)) {
-                    const float alpha = na / denom;
-                    const float beta = nb / denom;
-                    if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
-                        const int px = ((yi0 + iy) - y0) + ((xi0 + ix) - x0) * DIM;
-                        if (px < 0 || px >= NPIX) flags |= FLAG_OUT_OF_DOMAIN;
-                        emit(ridx, (uint32_t)(uint16_t)px, alpha, beta);
-                        ridx++;
-                    }
-                }
+                const int k = 2 * ix + iy;
+                const float d20 = p0x[ix] + p0y[iy];
+                const float d21 = p1x[ix] + p1y[iy];
+                na[k] = d11 * d20 - d01 * d21;
+                nb[k] = d00 * d21 - d01 * d20;
+                const bool sa = dpos ? na[k] > 0.0f : na[k] < 0.0f;
+                const bool sb = dpos ? nb[k] > 0.0f : nb[k] < 0.0f;
+                const bool c = okx[ix] && oky[iy] && sa && sb && !sum_exceeds_one(na[k], nb[k], denom, dpos);
+                cand |= c ? (1u << k) : 0u;
+            }
+        while (cand) {
+            const int k = __ffs(cand) - 1;
+            cand &= cand - 1;
+            const float nak = k == 0 ? na[0] : k == 1 ? na[1] : k == 2 ? na[2] : na[3];
+            const float nbk = k == 0 ? nb[0] : k == 1 ? nb[1] : k == 2 ? nb[2] : nb[3];
+            const float alpha = nak / denom;
+            const float beta = nbk / denom;
+            if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
+                const int px = ((yi0 + (k & 1)) - y0) + ((xi0 + (k >> 1)) - x0) * DIM;
+                if (px < 0 || px >= NPIX) flags |= FLAG_OUT_OF_DOMAIN;
+                emit(ridx, (uint32_t)(uint16_t)px, alpha, beta);
+                ridx++;
             }
         }
         return ridx;
@@ -552,6 +582,7 @@ __device__ __forceinline__ int tri_samples(float bx, float by, float cx, float c
             if (!(dpos ? na > 0.0f : na < 0.0f)) continue;
             const float nb = d00 * d21 - d01 * d20;
             if (!(dpos ? nb > 0.0f : nb < 0.0f)) continue;
+            if (sum_exceeds_one(na, nb, denom, dpos)) continue;
             const float alpha = na / denom;
             const float beta = nb / denom;
             if (alpha > 0 && beta > 0 && (alpha + beta <= 1)) {
