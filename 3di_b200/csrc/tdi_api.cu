@@ -279,7 +279,7 @@ struct Launch {
     size_t smem_neigh() const { return neigh_smem(); }
     size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * NE_PD * sizeof(double); }
     size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
-    size_t smem_solve() const { return (size_t)(m.KT * m.KT + m.KT) * sizeof(double); }
+    size_t smem_solve() const { return solve_smem(m.KT); }
     dim3 fblocks() const { return dim3((F + 127) / 128); }
     int A() const { return b.nact; }                      // frames active this round
     dim3 ablocks() const { return dim3((A() + 127) / 128); }
@@ -393,7 +393,7 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
     }
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
-    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(256), L.smem_solve(), L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(SV_THREADS), L.smem_solve(), L.s, L.m, L.b, c, stage));
     return TDI_OK;
 }
 

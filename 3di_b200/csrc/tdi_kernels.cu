@@ -1936,89 +1936,166 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
 }
 
 // ------------------------------------------------------------------------------------------
-// FP64 Cholesky solve (solver.h:70-105) of the shape system, one block per frame, then the
-// first trial of the line search. Column j: diagonal by one thread, then the rows below in
-// parallel, each a sequential dot product over k (the oracle's order).
+// FP64 Cholesky solve (solver.h:70-105, cuSOLVER DPOTRF/DPOTRS in the reference) of the shape
+// system, one block per frame, then the first trial of the line search.
+//
+// The lower triangle is held in registers: thread (tr, tc) = (tid % 16, tid / 16) owns the
+// entries (i, l) with i = tr + 16a, l = tc + 16b, i >= l. Step j: the pivot's owner takes the
+// square root; threads j+1..n-1 each divide one entry of column j (its owner left the
+// updated value in shared memory during the previous step); every thread then subtracts
+// L(i,j) L(l,j) from its entries right of column j. Each entry so receives its updates in
+// increasing j, the same sequence of subtractions as the oracle's left-looking dot products.
+// The forward substitution rides along (thread j divides y_j at step j, threads i > j then
+// update y_i, terms in increasing k); the back substitution runs by columns with terms in
+// decreasing k (the oracle's order), y_i held by thread i. Two barriers per factor step, one
+// per back step.
 
-// FP64 Cholesky factor and solve of one frame's system by the whole block (solver.h:70-105
-// with cuSOLVER DPOTRF/DPOTRS in the reference). L is column-major [n][n], holding H on entry.
-// Right-looking: after column j is scaled, every trailing entry is updated at once; each
-// entry receives its updates in increasing j, i.e. the same sequence of subtractions as the
-// left-looking dot products of the oracle. Forward substitution by columns (terms in
-// increasing k), back substitution by columns (terms in decreasing k, the oracle's order).
-// Every thread recomputes the pivot it needs, so a step costs one or two barriers.
-__device__ int chol_solve_block(double *L, int n, const float *g, double *y)
+constexpr int SV_THREADS = 256;
+constexpr int SV_MAXN = 128;
+
+__host__ __device__ __forceinline__ size_t solve_smem(int n)
 {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, nw = nt >> 5;
-    for (int j = 0; j < n; ++j) {
-        const double s = L[j * n + j];
-        if (!(s > 0.0)) return 0;               // every thread sees the same pivot
-        const double ljj = sqrt(s);
-        for (int i = j + 1 + tid; i < n; i += nt) L[j * n + i] = L[j * n + i] / ljj;
-        __syncthreads();
-        if (tid == 0) L[j * n + j] = ljj;
-        // trailing update of the lower triangle, entries (i, l) with j < l <= i < n: warps
-        // take columns l, lanes take rows i
-        for (int l = j + 1 + (tid >> 5); l < n; l += nw) {
-            const double llj = L[j * n + l];
-            for (int i = l + lane; i < n; i += 32) L[l * n + i] -= L[j * n + i] * llj;
-        }
-        __syncthreads();
-    }
-    for (int i = tid; i < n; i += nt) y[i] = (double)g[i];
-    __syncthreads();
-    for (int k = 0; k < n; ++k) {
-        const double yk = y[k] / L[k * n + k];
-        for (int i = k + 1 + tid; i < n; i += nt) y[i] -= L[k * n + i] * yk;
-        __syncthreads();
-        if (tid == 0) y[k] = yk;
-    }
-    __syncthreads();
-    for (int k = n - 1; k >= 0; --k) {
-        const double yk = y[k] / L[k * n + k];
-        for (int i = tid; i < k; i += nt) y[i] -= L[i * n + k] * yk;
-        __syncthreads();
-        if (tid == 0) y[k] = yk;
-    }
-    __syncthreads();
-    return 1;
+    return ((size_t)n * n + 4 * SV_MAXN + 2) * sizeof(double);
 }
 
-__global__ void __launch_bounds__(256) k_solve(DModel m, DBatch b, Cfg c, int stage)
+template <int RB>
+__device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, const Cfg &c, int stage, int f,
+                                            FrameCtl &ctl, double *sm)
+{
+    const int n = m.KT, KTP = m.KTP, K = m.K;
+    const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+    double *Lf = sm;                     // [n][n] column-major: the factor, for the back steps
+    double *raw = Lf + (size_t)n * n;    // column j before its scaling
+    double *col = raw + SV_MAXN;         // column j after its scaling
+    double *yv = col + SV_MAXN;          // forward results y_j / L(j,j)
+    double *yb = yv + SV_MAXN;           // back results
+    double *piv = yb + SV_MAXN;          // [0] pivot, [1] failure flag
+    const float *H = b.H + (size_t)f * KTP * KTP;
+    const float *gv = b.g + (size_t)f * KTP;
+    double v[RB][RB];
+#pragma unroll
+    for (int a = 0; a < RB; ++a)
+#pragma unroll
+        for (int bb = 0; bb < RB; ++bb) {
+            const int i = tr + 16 * a, l = tc + 16 * bb;
+            v[a][bb] = (i < n && l < n && i >= l) ? (double)H[(size_t)l * KTP + i] : 0.0;
+        }
+    double y = tid < n ? (double)gv[tid] : 0.0;
+    if (tid == 0) piv[1] = 0.0;
+    // column 0 before scaling
+#pragma unroll
+    for (int a = 0; a < RB; ++a)
+        if (tc == 0 && tr + 16 * a < n) raw[tr + 16 * a] = v[a][0];
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        const int jt = j & 15, jb = j >> 4;
+        if (tr == jt && tc == jt) {                  // the pivot's owner
+#pragma unroll
+            for (int a = 0; a < RB; ++a)
+                if (a == jb) {
+                    const double s = v[a][a];
+                    if (!(s > 0.0)) piv[1] = 1.0;
+                    const double ljj = sqrt(s);
+                    piv[0] = ljj;
+                    Lf[(size_t)j * n + j] = ljj;
+                }
+        }
+        __syncthreads();
+        if (piv[1] != 0.0) {                         // block-uniform: the pivot was not positive
+            float *d = b.d + (size_t)f * KTP;
+            for (int i = tid; i < n; i += SV_THREADS) d[i] = __int_as_float(0x7fc00000);
+            if (tid == 0) {
+                ctl.flags |= FLAG_CHOL_FAILED | FLAG_NAN_DIRECTION;
+                end_shape_stage(c, ctl, stage, ctl.outer);
+            }
+            return;
+        }
+        const double ljj = piv[0];
+        if (tid > j && tid < n) {
+            const double lij = raw[tid] / ljj;
+            col[tid] = lij;
+            Lf[(size_t)j * n + tid] = lij;
+        }
+        if (tid == j) { y = y / ljj; yv[j] = y; }
+        __syncthreads();
+        // trailing update of the owned entries right of column j
+        double ci[RB], cl[RB];
+#pragma unroll
+        for (int a = 0; a < RB; ++a) {
+            const int i = tr + 16 * a, l = tc + 16 * a;
+            ci[a] = (i > j && i < n) ? col[i] : 0.0;
+            cl[a] = (l > j && l < n) ? col[l] : 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < RB; ++a)
+#pragma unroll
+            for (int bb = 0; bb < RB; ++bb) {
+                const int i = tr + 16 * a, l = tc + 16 * bb;
+                if (l > j && i >= l && i < n) v[a][bb] -= ci[a] * cl[bb];
+            }
+        if (tid > j && tid < n) y -= col[tid] * yv[j];
+        // the next column before its scaling
+        const int jn = j + 1;
+        if (jn < n && tc == (jn & 15)) {
+#pragma unroll
+            for (int a = 0; a < RB; ++a)
+#pragma unroll
+                for (int bb = 0; bb < RB; ++bb)
+                    if (bb == (jn >> 4)) {
+                        const int i = tr + 16 * a;
+                        if (i > jn && i < n) raw[i] = v[a][bb];
+                    }
+        }
+    }
+    __syncthreads();
+    // back substitution: y_k / L(k,k), then y_i -= L(k,i) y_k for i < k
+    for (int k = n - 1; k >= 0; --k) {
+        if (tid == k) { y = y / Lf[(size_t)k * n + k]; yb[k] = y; }
+        __syncthreads();
+        if (tid < k) y -= Lf[(size_t)tid * n + k] * yb[k];
+    }
+    // direction, its slope and the first trial point
+    float *d = b.d + (size_t)f * KTP;
+    float *dsm = reinterpret_cast<float *>(raw);
+    if (tid < n) { const float dv = (float)(-y); d[tid] = dv; dsm[tid] = dv; }
+    __syncthreads();
+    if (isnan(dsm[0])) {
+        if (tid == 0) {
+            ctl.flags |= FLAG_NAN_DIRECTION;
+            end_shape_stage(c, ctl, stage, ctl.outer);
+        }
+        return;
+    }
+    const int n_upd = stage == ST_FINETUNE ? K : n;
+    const float t = 1.0f;
+    const float *x = b.x + (size_t)f * KTP;
+    float *xl = b.x_ls + (size_t)f * KTP;
+    for (int a = tid; a < n_upd; a += SV_THREADS) xl[a] = x[a] + t * dsm[a];
+    if (tid == 0) {
+        double dg = 0.0;
+        for (int a = 0; a < n; ++a) dg += (double)dsm[a] * (double)gv[a];
+        ctl.l2base = (float)dg;
+        ctl.mode = M_TRIAL;
+        ctl.t = t;
+        const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
+        // the trial's tau_z (left as it was when the stage does not update the pose)
+        const float tz = n_upd > K + 2 ? x[K + 2] + t * dsm[K + 2] : xl[K + 2];
+        if (tz < 0.0f) {
+            ctl.flags |= FLAG_STUCK_NEG_TZ;
+            end_shape_stage(c, ctl, stage, maxit);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(SV_THREADS) k_solve(DModel m, DBatch b, Cfg c, int stage)
 {
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
     if (threadIdx.x == 0) prof_count(b, KID_SOLVE);
     extern __shared__ double ssm[];
-    const int KT = m.KT, KTP = m.KTP;
-    double *L = ssm;             // [KT][KT]
-    double *y = L + KT * KT;     // [KT]
-    const float *H = b.H + (size_t)f * KTP * KTP;
-    for (int col = threadIdx.x >> 5; col < KT; col += blockDim.x >> 5)
-        for (int row = threadIdx.x & 31; row < KT; row += 32) L[col * KT + row] = (double)H[(size_t)col * KTP + row];
-    __syncthreads();
-    const float *gv = b.g + (size_t)f * KTP;
-    const int ok = chol_solve_block(L, KT, gv, y);
-    if (threadIdx.x != 0) return;
-    float *d = b.d + (size_t)f * KTP;
-    if (ok) { for (int i = 0; i < KT; ++i) d[i] = (float)(-y[i]); }
-    else { for (int i = 0; i < KT; ++i) d[i] = __int_as_float(0x7fc00000); ctl.flags |= FLAG_CHOL_FAILED; }
-    if (isnan(d[0])) {
-        ctl.flags |= FLAG_NAN_DIRECTION;
-        end_shape_stage(c, ctl, stage, ctl.outer);
-        return;
-    }
-    double dg = 0.0;
-    for (int a = 0; a < KT; ++a) dg += (double)d[a] * (double)gv[a];
-    ctl.l2base = (float)dg;
-    ctl.mode = M_TRIAL;
-    ctl.t = 1.0f;
-    const int maxit = stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune;
-    if (!set_trial(m, b, f, stage == ST_FINETUNE ? m.K : m.KT)) {
-        ctl.flags |= FLAG_STUCK_NEG_TZ;
-        end_shape_stage(c, ctl, stage, maxit);
-    }
+    if (m.KT <= 96) solve_frame<6>(m, b, c, stage, f, ctl, ssm);
+    else solve_frame<8>(m, b, c, stage, f, ctl, ssm);
 }
 
 // ------------------------------------------------------------------------------------------
