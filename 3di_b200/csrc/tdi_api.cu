@@ -269,6 +269,20 @@ dim3 vertex_grid(const DModel &m, int frames)
     return dim3((unsigned)std::max(ftiles, std::min((long)VT_BLOCKS_PER_SM * sms, ftiles * ntiles)));
 }
 
+// Blocks per frame of the depth pass: 16, or more when few frames run, so that a short
+// launch still spreads over every SM (about five resident blocks per SM).
+unsigned raster_blocks(int frames)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    const int want = (5 * sms + std::max(frames, 1) - 1) / std::max(frames, 1);
+    return (unsigned)std::max(RD_BLOCKS, std::min(RD_MAX_BLOCKS, want));
+}
+
 struct Launch {
     tdi_batch *bt;
     const DModel &m;
@@ -361,8 +375,8 @@ tdi_status geometry(const Launch &L, const Cfg &c, int stage)
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
                    (size_t)PC_WARPS * (2 * L.m.K + 4 * NL + NL * PC_LM) * sizeof(float), L.s, L.m, L.b, c, stage));
     TDI_TRY(launch(L.bt, 0, k_compact_render, dim3(1), dim3(1024), 0, L.s, L.b));
-    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, 8), L.smem_vertex(), L.s, L.m, L.b));
-    TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, VT_WARPS + 1), L.smem_vertex(), L.s, L.m, L.b));
+    TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(raster_blocks(L.A()), L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RESOLVE, k_raster_resolve, dim3(L.A()), dim3(RR_THREADS), 0, L.s, L.m, L.b));
     return TDI_OK;
 }
@@ -916,7 +930,7 @@ tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const 
     TDI_CUDA(cudaMemcpy(d.act, &frame, sizeof(int32_t), cudaMemcpyHostToDevice));
     d.nact = 1;
     TDI_TRY(launch(b, 0, k_set_render, dim3(1), dim3(256), 0, (cudaStream_t)0, d, (int)frame));
-    TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, 1), dim3(RD_THREADS), 0, (cudaStream_t)0, m, d));
+    TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(raster_blocks(1), 1), dim3(RD_THREADS), 0, (cudaStream_t)0, m, d));
     TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(1), dim3(RR_THREADS), 0, (cudaStream_t)0, m, d));
     TDI_CUDA(cudaDeviceSynchronize());
     FrameCtl ctl;
@@ -943,8 +957,8 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     if (n > 0) {
         TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
         TDI_TRY(launch(b, 0, k_compact_render, dim3(1), dim3(1024), 0, s, (const DBatch)d));
-        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, 8), L.smem_vertex(), s, m, d));
-        TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(RD_BLOCKS, n), dim3(RD_THREADS), 0, s, m, d));
+        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, VT_WARPS + 1), L.smem_vertex(), s, m, d));
+        TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(raster_blocks(n), n), dim3(RD_THREADS), 0, s, m, d));
         TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));
     }
     float *img = d.img;                                   // [F][NPIX] image, then [F][NPIX] map

@@ -184,6 +184,8 @@ constexpr int VT_V = 32;                                   // vertices per tile 
 constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
 constexpr int VT_FR = 16;                                   // per-frame floats: R(9), tau(3), cam(4)
 constexpr int VT_BLOCKS_PER_SM = 2;
+constexpr int VT_WARPS = 8;                                 // computing warps; one more issues the copies
+constexpr int VT_THREADS = (VT_WARPS + 1) * 32;
 
 __host__ __device__ __forceinline__ int vt_row(int KP) { return 3 * KP + 4; }   // basis row pitch (floats)
 __host__ __device__ __forceinline__ size_t vt_smem(int KP)
@@ -191,7 +193,7 @@ __host__ __device__ __forceinline__ size_t vt_smem(int KP)
     return ((size_t)2 * VT_V * vt_row(KP) + (size_t)VT_F * KP + (size_t)VT_F * VT_FR) * sizeof(float);
 }
 
-__global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBatch b)
+__global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBatch b)
 {
     extern __shared__ __align__(16) float vsm[];
     const int KP = m.KP, K = m.K, ER = vt_row(KP);
@@ -199,8 +201,10 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
     float *Xs = Eb + 2 * VT_V * ER;            // [VT_F][KP]: coefficients per frame
     float *Fs = Xs + VT_F * KP;                // [VT_F][VT_FR]
     __shared__ int s_any;
+    __shared__ volatile int s_abort;
+    __shared__ int s_issued;
     __shared__ int s_render[VT_F], s_frame[VT_F];
-    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
     const int ntiles = (m.V + VT_V - 1) / VT_V;
     const int rc = b.rcount[0];
     const int ftiles = (rc + VT_F - 1) / VT_F;
@@ -210,7 +214,8 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
     const int gy = blockIdx.x / ftiles;        // vertex-tile stripe
     const int f0 = (blockIdx.x - gy * ftiles) * VT_F;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    if (tid == 0) s_any = 0;
+    const bool producer = threadIdx.y == VT_WARPS;
+    if (tid == 0) { s_any = 0; s_abort = 0; s_issued = 0; }
     __syncthreads();
     if (tid < VT_F) {
         const int ai = f0 + tid;
@@ -223,113 +228,140 @@ __global__ void __launch_bounds__(256, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBat
             if (gy == 0) prof_count(b, KID_VERTEX);
         }
     }
+    if (tid == 0) {
+        mbar_init(smem_addr(&s_full[0]), 1);
+        mbar_init(smem_addr(&s_full[1]), 1);
+        mbar_init(smem_addr(&s_empty[0]), VT_WARPS);
+        mbar_init(smem_addr(&s_empty[1]), VT_WARPS);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     if (!s_any) return;
     const int rowbytes = 3 * KP * (int)sizeof(float);
     const uint32_t eb_addr = smem_addr(Eb);
-    auto issue = [&](int j) {                  // thread 0: tile j of this block into buffer j & 1
-        const int t = gy + j * groups;
-        if (t >= ntiles) return;
-        const int nv = min(VT_V, m.V - t * VT_V), buf = j & 1;
-        const uint32_t bar = smem_addr(&s_bar[buf]);
-        mbar_expect_tx(bar, (uint32_t)(nv * rowbytes));
-        for (int r = 0; r < nv; ++r)
-            bulk_g2s(eb_addr + (uint32_t)((buf * VT_V + r) * ER) * 4u, m.E + (size_t)(t * VT_V + r) * 3 * KP,
-                     (uint32_t)rowbytes, bar);
-    };
-    if (tid == 0) {
-        mbar_init(smem_addr(&s_bar[0]), 1);
-        mbar_init(smem_addr(&s_bar[1]), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        issue(0);
-        issue(1);
-    }
-    for (int fl = threadIdx.y; fl < VT_F; fl += 8) {
-        const int f = s_frame[fl];
-        const float *xr = f >= 0 ? b.xe + (size_t)f * m.KTP : nullptr;
-        for (int k = threadIdx.x; k < KP; k += 32) Xs[fl * KP + k] = (xr && k < K) ? xr[k] : 0.0f;
-        if (threadIdx.x < VT_FR) {
-            const int i = threadIdx.x;
-            float v = 0.0f;
-            if (f >= 0) v = i < 9 ? b.R[f * 9 + i] : i < 12 ? b.xe[(size_t)f * m.KTP + K + (i - 9)] : b.cam[f * 4 + (i - 12)];
-            Fs[fl * VT_FR + i] = v;
+    if (!producer) {
+        for (int fl = threadIdx.y; fl < VT_F; fl += VT_WARPS) {
+            const int f = s_frame[fl];
+            const float *xr = f >= 0 ? b.xe + (size_t)f * m.KTP : nullptr;
+            for (int k = threadIdx.x; k < KP; k += 32) Xs[fl * KP + k] = (xr && k < K) ? xr[k] : 0.0f;
+            if (threadIdx.x < VT_FR) {
+                const int i = threadIdx.x;
+                float v = 0.0f;
+                if (f >= 0) v = i < 9 ? b.R[f * 9 + i] : i < 12 ? b.xe[(size_t)f * m.KTP + K + (i - 9)] : b.cam[f * 4 + (i - 12)];
+                Fs[fl * VT_FR + i] = v;
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        // the first two tiles stream in while the coefficients are staged
+        for (int j = 0; j < 2; ++j) {
+            const int t = gy + j * groups;
+            if (t >= ntiles) break;
+            const int nv = min(VT_V, m.V - t * VT_V);
+            const uint32_t bar = smem_addr(&s_full[j]);
+            mbar_expect_tx(bar, (uint32_t)(nv * rowbytes));
+            for (int r = 0; r < nv; ++r)
+                bulk_g2s(eb_addr + (uint32_t)((j * VT_V + r) * ER) * 4u, m.E + (size_t)(t * VT_V + r) * 3 * KP,
+                         (uint32_t)rowbytes, bar);
         }
     }
-    __syncthreads();
-    const int vl = threadIdx.x;
-    const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
-    int j = 0;
-    bool ok = true;
-    for (;; ++j) {
-        const int t = gy + j * groups;
-        if (t >= ntiles) break;
-        const int buf = j & 1;
-        const bool w = mbar_wait(smem_addr(&s_bar[buf]), (uint32_t)((j >> 1) & 1));
-        if (!__syncthreads_and(w)) { ok = false; break; }
-        const float *er = Eb + (size_t)(buf * VT_V + vl) * ER;
-        float acc[VT_FPT][3];
+    __syncthreads();                           // coefficients staged
+    if (producer) {
+        if (threadIdx.x == 0) {
+            // tile j into buffer j & 1 once the computing warps have released tile j - 2
+            int j = 2;
+            for (;; ++j) {
+                const int t = gy + j * groups;
+                if (t >= ntiles || s_abort) break;
+                const int buf = j & 1;
+                if (!mbar_wait(smem_addr(&s_empty[buf]), (uint32_t)(((j - 2) >> 1) & 1))) {
+                    s_abort = 1;
+                    atomicOr(b.err, 2);
+                    break;
+                }
+                const int nv = min(VT_V, m.V - t * VT_V);
+                const uint32_t bar = smem_addr(&s_full[buf]);
+                mbar_expect_tx(bar, (uint32_t)(nv * rowbytes));
+                for (int r = 0; r < nv; ++r)
+                    bulk_g2s(eb_addr + (uint32_t)((buf * VT_V + r) * ER) * 4u, m.E + (size_t)(t * VT_V + r) * 3 * KP,
+                             (uint32_t)rowbytes, bar);
+            }
+            s_issued = min(j, (ntiles - gy + groups - 1) / groups);
+        }
+    } else {
+        const int vl = threadIdx.x;
+        const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
+        for (int j = 0;; ++j) {
+            const int t = gy + j * groups;
+            if (t >= ntiles) break;
+            const int buf = j & 1;
+            const int v = t * VT_V + vl;
+            // the epilogue's per-vertex inputs, loaded before the wait
+            float mx = 0.0f, my = 0.0f, mz = 0.0f, tx = 0.0f;
+            if (v < m.V) { mx = m.mean[v]; my = m.mean[m.V + v]; mz = m.mean[2 * m.V + v]; tx = m.tex[v]; }
+            const bool w = mbar_wait(smem_addr(&s_full[buf]), (uint32_t)((j >> 1) & 1));
+            if (!__all_sync(0xffffffffu, w)) {
+                if (threadIdx.x == 0) { s_abort = 1; atomicOr(b.err, 2); }
+                break;
+            }
+            const float *er = Eb + (size_t)(buf * VT_V + vl) * ER;
+            float acc[VT_FPT][3];
 #pragma unroll
-        for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
-        // sequential fused multiply-add over k for every output (the order the oracle uses)
-        int k = 0;
-        for (; k + 4 <= K; k += 4) {
-            const float4 ex = *reinterpret_cast<const float4 *>(er + k);
-            const float4 ey = *reinterpret_cast<const float4 *>(er + KP + k);
-            const float4 ez = *reinterpret_cast<const float4 *>(er + 2 * KP + k);
-            const float exv[4] = {ex.x, ex.y, ex.z, ex.w}, eyv[4] = {ey.x, ey.y, ey.z, ey.w};
-            const float ezv[4] = {ez.x, ez.y, ez.z, ez.w};
+            for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
+            // sequential fused multiply-add over k for every output (the order the oracle uses)
+            int k = 0;
+            for (; k + 4 <= K; k += 4) {
+                const float4 ex = *reinterpret_cast<const float4 *>(er + k);
+                const float4 ey = *reinterpret_cast<const float4 *>(er + KP + k);
+                const float4 ez = *reinterpret_cast<const float4 *>(er + 2 * KP + k);
+                const float exv[4] = {ex.x, ex.y, ex.z, ex.w}, eyv[4] = {ey.x, ey.y, ey.z, ey.w};
+                const float ezv[4] = {ez.x, ez.y, ez.z, ez.w};
 #pragma unroll
-            for (int q = 0; q < VT_FPT; ++q) {
-                const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
-                const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
+                for (int q = 0; q < VT_FPT; ++q) {
+                    const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
+                    const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
-                for (int jj = 0; jj < 4; ++jj) {
-                    acc[q][0] = fmaf(exv[jj], xv[jj], acc[q][0]);
-                    acc[q][1] = fmaf(eyv[jj], xv[jj], acc[q][1]);
-                    acc[q][2] = fmaf(ezv[jj], xv[jj], acc[q][2]);
+                    for (int jj = 0; jj < 4; ++jj) {
+                        acc[q][0] = fmaf(exv[jj], xv[jj], acc[q][0]);
+                        acc[q][1] = fmaf(eyv[jj], xv[jj], acc[q][1]);
+                        acc[q][2] = fmaf(ezv[jj], xv[jj], acc[q][2]);
+                    }
+                }
+            }
+            for (; k < K; ++k) {
+                const float ex = er[k], ey = er[KP + k], ez = er[2 * KP + k];
+#pragma unroll
+                for (int q = 0; q < VT_FPT; ++q) {
+                    const float xv = xr[q * KP + k];
+                    acc[q][0] = fmaf(ex, xv, acc[q][0]);
+                    acc[q][1] = fmaf(ey, xv, acc[q][1]);
+                    acc[q][2] = fmaf(ez, xv, acc[q][2]);
+                }
+            }
+            __syncwarp();                          // this warp is done with the buffer
+            if (threadIdx.x == 0) mbar_arrive(smem_addr(&s_empty[buf]));
+            if (v < m.V) {
+#pragma unroll
+                for (int q = 0; q < VT_FPT; ++q) {
+                    const int fl = threadIdx.y * VT_FPT + q;
+                    if (!s_render[fl]) continue;
+                    const int f = s_frame[fl];
+                    const float *R = Fs + fl * VT_FR, *tau = R + 9, *cam = R + 12;
+                    const float X0 = mx + acc[q][0], Y0 = my + acc[q][1], Z0 = mz + acc[q][2];
+                    const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
+                    const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
+                    const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
+                    b.geo[(size_t)f * m.V + v] = make_float4(X0, Y0, Z0, tx);
+                    b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
                 }
             }
         }
-        for (; k < K; ++k) {
-            const float ex = er[k], ey = er[KP + k], ez = er[2 * KP + k];
-#pragma unroll
-            for (int q = 0; q < VT_FPT; ++q) {
-                const float xv = xr[q * KP + k];
-                acc[q][0] = fmaf(ex, xv, acc[q][0]);
-                acc[q][1] = fmaf(ey, xv, acc[q][1]);
-                acc[q][2] = fmaf(ez, xv, acc[q][2]);
-            }
-        }
-        const int v = t * VT_V + vl;
-        if (v < m.V) {
-            const float mx = m.mean[v], my = m.mean[m.V + v], mz = m.mean[2 * m.V + v], tx = m.tex[v];
-#pragma unroll
-            for (int q = 0; q < VT_FPT; ++q) {
-                const int fl = threadIdx.y * VT_FPT + q;
-                if (!s_render[fl]) continue;
-                const int f = s_frame[fl];
-                const float *R = Fs + fl * VT_FR, *tau = R + 9, *cam = R + 12;
-                const float X0 = mx + acc[q][0], Y0 = my + acc[q][1], Z0 = mz + acc[q][2];
-                const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
-                const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
-                const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];
-                b.geo[(size_t)f * m.V + v] = make_float4(X0, Y0, Z0, tx);
-                b.proj[(size_t)f * m.V + v] = make_float4((cam[0] * X3) / Z3 + cam[2], (cam[1] * Y3) / Z3 + cam[3], Z3, 0.0f);
-            }
-        }
-        __syncthreads();                       // every thread is done with this buffer
-        if (tid == 0) issue(j + 2);
     }
-    if (!ok) {
-        // copies of tiles j and j + 1 may still be in flight: wait for them (bounded) before
-        // the block's shared memory is released
-        if (tid == 0) {
-            atomicOr(b.err, 2);
-            mbar_wait(smem_addr(&s_bar[j & 1]), (uint32_t)((j >> 1) & 1));
-            if (gy + (j + 1) * groups < ntiles)
-                mbar_wait(smem_addr(&s_bar[(j + 1) & 1]), (uint32_t)(((j + 1) >> 1) & 1));
-        }
-        __syncthreads();
+    __syncthreads();
+    if (s_abort && tid == VT_WARPS * 32) {
+        // copies of the last two issued tiles may still be in flight: wait for them (bounded)
+        // before the block's shared memory is released
+        for (int j = max(0, s_issued - 2); j < s_issued; ++j)
+            mbar_wait(smem_addr(&s_full[j & 1]), (uint32_t)((j >> 1) & 1));
     }
 }
 
@@ -629,7 +661,8 @@ __device__ __forceinline__ bool survives(unsigned long long k, uint32_t tag, uin
 }
 
 constexpr int RD_THREADS = 256;             // depth pass: threads per block
-constexpr int RD_BLOCKS = 16;               // depth pass: blocks per frame
+constexpr int RD_BLOCKS = 16;               // depth pass: blocks per frame (at least)
+constexpr int RD_MAX_BLOCKS = 256;          // depth pass: blocks per frame when few frames render
 constexpr int RR_THREADS = 1024;            // resolve: one block per frame
 constexpr int RR_WARPS = RR_THREADS / 32;
 
@@ -646,7 +679,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_raster_depth(DModel m, DBatch b)
     const int x0 = b.x0y0[2 * f], y0 = b.x0y0[2 * f + 1];
     const int T = m.T;
     // each block a contiguous range of the Morton order
-    const int per_block = (T + RD_BLOCKS - 1) / RD_BLOCKS;
+    const int per_block = (T + gridDim.x - 1) / gridDim.x;
     const int s_begin = blockIdx.x * per_block, s_end = min(T, s_begin + per_block);
     uint32_t flags = 0;
     for (int s = s_begin + (int)threadIdx.x; s < s_end; s += RD_THREADS) {
