@@ -162,7 +162,10 @@ struct tdi_batch {
 
 namespace {
 
-constexpr int FIT_LANES = 2;       // streams a batched fit runs on
+// Streams a batched fit runs on. Two lanes (halves of the batch on two streams) measured
+// slower than one on B200 once the per-frame kernels filled the SMs by themselves: 3,235
+// against 3,437 frames/s on the 1,024-frame video fit, so the batch runs as one lane.
+constexpr int FIT_LANES = 1;
 constexpr int FIT_LANE_MIN = 32;   // frames a lane needs before a batch is split
 
 template <typename T>
