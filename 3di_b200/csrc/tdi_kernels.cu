@@ -914,7 +914,7 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
 // and the correlation sum.
 
 struct Shading {
-    float tex, Id, nn[3], p[3], v[3];
+    float tex, Id, t, nn[3], p[3], v[3];
 };
 
 __device__ __forceinline__ void camera_coords(const float *R, const float *tau, float X0, float Y0,
@@ -952,6 +952,7 @@ __device__ __forceinline__ Shading shade(const DModel &m, const float4 *geo, con
                + s.nn[2] * ((R[6] * d0 + R[7] * d1) + R[8] * d2);
     Id = Id - ((s.nn[0] * s.p[0] + s.nn[1] * s.p[1]) + s.nn[2] * s.p[2]);
     const float t = (gb.w * al + gc.w * be) + ga4.w * ga;
+    s.t = t;
     s.tex = t + (Lint * t) * Id;
     s.Id = Id;
     float bX, bY, bZ, cX, cY, cZ, aX, aY, aZ;
@@ -2135,6 +2136,8 @@ __global__ void __launch_bounds__(SV_THREADS) k_solve(DModel m, DBatch b, Cfg c,
 // Light system (derivative_computer.cu:235-312): dI/dlambda = L t (R n), chain rule, 3x3
 // normal equations in FP64, Cholesky, first trial. One block per frame.
 
+constexpr int LJ_U = 4;   // fragments per thread whose gathers are in flight together
+
 __global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
 {
     const int f = b.act[blockIdx.x];
@@ -2151,32 +2154,64 @@ __global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
     const float Lint = b.Lint[f];
     const Fragment *frags = b.frag + (size_t)f * NMAX;
     float *Jl = b.J + (size_t)f * NMAX * m.KTP;   // rows of pitch 4
-    for (int n = tid; n < N; n += 256) {
-        const Shading s = shade(m, geo, frags[n], R, tau, lam, Lint);
-        const Fragment fr = frags[n];
-        const int tri = fr.tri;
-        const float al = fr.al, be = fr.be, ga = (1 - fr.al) - fr.be;
-        const int4 tc = __ldg(m.tl4 + tri);
-        const float t = (geo[tc.x].w * al + geo[tc.y].w * be) + geo[tc.z].w * ga;
-        const float Lt = Lint * t;
-        const float r0 = Lt * s.nn[0], r1 = Lt * s.nn[1], r2 = Lt * s.nn[2];
-        for (int j = 0; j < 3; ++j) Jl[(size_t)n * 4 + j] = (r0 * R[j] + r1 * R[j + 3]) + r2 * R[j + 6];
-        Jl[(size_t)n * 4 + 3] = 0.0f;
+    // fragments LJ_U at a time, their gathers issued together (each thread still takes its
+    // fragments in ascending order, so the FP64 sums below keep their order)
+    for (int n0 = tid; n0 < N; n0 += 256 * LJ_U) {
+        Fragment fr[LJ_U];
+#pragma unroll
+        for (int u = 0; u < LJ_U; ++u) {
+            const int n = n0 + u * 256;
+            fr[u] = n < N ? frags[n] : Fragment{0u, 0, 0.0f, 0.0f};
+        }
+        float rr[LJ_U][3];
+#pragma unroll
+        for (int u = 0; u < LJ_U; ++u) {
+            const Shading sh = shade(m, geo, fr[u], R, tau, lam, Lint);
+            const float Lt = Lint * sh.t;
+            const float r0 = Lt * sh.nn[0], r1 = Lt * sh.nn[1], r2 = Lt * sh.nn[2];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) rr[u][j] = (r0 * R[j] + r1 * R[j + 3]) + r2 * R[j + 6];
+        }
+#pragma unroll
+        for (int u = 0; u < LJ_U; ++u) {
+            const int n = n0 + u * 256;
+            if (n >= N) break;
+            *reinterpret_cast<float4 *>(Jl + (size_t)n * 4) = make_float4(rr[u][0], rr[u][1], rr[u][2], 0.0f);
+        }
     }
     __syncthreads();
     const int32_t *nb = b.nb + (size_t)f * 4 * NMAX;
     const float *fg = b.fgrad + (size_t)f * 5 * NMAX;
     double acc[12];
     for (int q = 0; q < 12; ++q) acc[q] = 0.0;
-    for (int n = tid; n < N; n += 256) {
-        const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
-        const float pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
-        float ox[3], oy[3];
-        for (int j = 0; j < 3; ++j) chain(Jl, 4, nb, n, j, gx, gy, pre, ox[j], oy[j]);
-        const double sx = fg[3 * NMAX + n], sy = fg[4 * NMAX + n];
-        for (int a = 0; a < 3; ++a) {
-            acc[9 + a] += sx * ox[a] + sy * oy[a];
-            for (int bb = 0; bb < 3; ++bb) acc[a * 3 + bb] += (double)ox[a] * ox[bb] + (double)oy[a] * oy[bb];
+    for (int n0 = tid; n0 < N; n0 += 256 * LJ_U) {
+        float4 jr[LJ_U][4];
+#pragma unroll
+        for (int u = 0; u < LJ_U; ++u) {
+            const int n = n0 + u * 256;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                jr[u][q] = n < N ? *reinterpret_cast<const float4 *>(Jl + (size_t)nb[q * NMAX + n] * 4) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < LJ_U; ++u) {
+            const int n = n0 + u * 256;
+            if (n >= N) break;
+            const float gx = fg[n], gy = fg[NMAX + n], h = fg[2 * NMAX + n];
+            const float pre = (float)(1.0 / (0.001 + (double)(h * h * h)));
+            float ox[3], oy[3];
+            const float k0[3] = {jr[u][0].x, jr[u][0].y, jr[u][0].z}, k1[3] = {jr[u][1].x, jr[u][1].y, jr[u][1].z};
+            const float k2[3] = {jr[u][2].x, jr[u][2].y, jr[u][2].z}, k3[3] = {jr[u][3].x, jr[u][3].y, jr[u][3].z};
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float vv[4] = {k0[j], k1[j], k2[j], k3[j]};
+                chain_value(vv, pre, 2 * gx, 2 * gy, ox[j], oy[j]);
+            }
+            const double sx = fg[3 * NMAX + n], sy = fg[4 * NMAX + n];
+            for (int a = 0; a < 3; ++a) {
+                acc[9 + a] += sx * ox[a] + sy * oy[a];
+                for (int bb = 0; bb < 3; ++bb) acc[a * 3 + bb] += (double)ox[a] * ox[bb] + (double)oy[a] * oy[bb];
+            }
         }
     }
     for (int q = 0; q < 12; ++q)
