@@ -32,7 +32,7 @@ FLAG_FAIL = 32
 FLAG_OVERFLOW = 64
 
 READ_FRAGMENTS, READ_NEIGHBOURS, READ_GRADIENTS, READ_JACOBIAN, READ_NORMAL_EQ, READ_SCALARS, \
-    READ_GEOMETRY = range(7)
+    READ_GEOMETRY, READ_CROP, READ_FRAME_DATA = range(9)
 
 
 class TdiError(RuntimeError):
@@ -51,6 +51,13 @@ class FramesDesc(C.Structure):
     _fields_ = [("n_frames", C.c_int32), ("targets", C.c_void_p), ("xl", C.c_void_p),
                 ("yl", C.c_void_p), ("bounds", C.c_void_p), ("face_size", C.c_void_p),
                 ("cam", C.c_void_p), ("x0y0", C.c_void_p)]
+
+
+class VideoFramesDesc(C.Structure):
+    _fields_ = [("n_frames", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
+                ("row_bytes", C.c_int64), ("bgr", C.c_void_p), ("xp", C.c_void_p), ("yp", C.c_void_p),
+                ("bounds", C.c_void_p), ("face_size", C.c_void_p), ("cam", C.c_void_p),
+                ("ref_face_size", C.c_float)]
 
 
 class FitConfig(C.Structure):
@@ -74,6 +81,7 @@ SIGNATURES = {
     "tdi_batch_create": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
     "tdi_batch_destroy": (C.c_int32, [C.c_void_p]),
     "tdi_batch_set_frames": (C.c_int32, [C.c_void_p, C.POINTER(FramesDesc), C.c_void_p]),
+    "tdi_batch_set_video_frames": (C.c_int32, [C.c_void_p, C.POINTER(VideoFramesDesc), C.c_void_p]),
     "tdi_batch_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_fit": (C.c_int32, [C.c_void_p, C.POINTER(FitConfig), C.c_void_p]),
     "tdi_batch_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -219,6 +227,22 @@ class Batch:
         _check(load_library().tdi_batch_set_frames(self.handle, C.byref(d), None))
         self.n = d.n_frames
 
+    def set_video_frames(self, bgr, xp, yp, bounds, face_size, cam, ref_face_size):
+        """Raw frames (the reference's decoded video frames): bgr [F][H][W][3] uint8 (or with a
+        row pitch: [F][H][row_bytes]), landmarks xp, yp [F][51] in image pixels, bounds
+        [F][4][51], face_size [F] in image pixels, cam [F][4] of the original camera. The
+        library rescales each frame by ref_face_size / face_size and forms the crops on the
+        device (tdi_batch_set_video_frames)."""
+        bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+        F, H = bgr.shape[0], bgr.shape[1]
+        row_bytes = int(np.prod(bgr.shape[2:]))
+        W = bgr.shape[2] if bgr.ndim == 4 else row_bytes // 3
+        xp, yp, bounds, face_size, cam = _f32(xp), _f32(yp), _f32(bounds), _f32(face_size), _f32(cam)
+        d = VideoFramesDesc(F, W, H, row_bytes, _p(bgr), _p(xp), _p(yp), _p(bounds), _p(face_size),
+                            _p(cam), float(ref_face_size))
+        _check(load_library().tdi_batch_set_video_frames(self.handle, C.byref(d), None))
+        self.n = F
+
     def set_state(self, x, lam, L):
         x, lam, L = _f32(x), _f32(lam), _f32(L)
         _check(load_library().tdi_batch_set_state(self.handle, _p(x), _p(lam), _p(L), None))
@@ -253,7 +277,7 @@ class Batch:
         KT = self.model.K + 6
         cap = {READ_FRAGMENTS: 4 * 32768, READ_NEIGHBOURS: 4 * 32768, READ_GRADIENTS: 5 * 32768,
                READ_JACOBIAN: 32768 * KT, READ_NORMAL_EQ: KT * KT + 2 * KT, READ_SCALARS: 4,
-               READ_GEOMETRY: 6 * self.model.V}[what]
+               READ_GEOMETRY: 6 * self.model.V, READ_CROP: NPIX, READ_FRAME_DATA: 2 * 51 + 7}[what]
         dt = np.float64 if what == READ_SCALARS else (np.int32 if what in (READ_FRAGMENTS, READ_NEIGHBOURS) else np.float32)
         buf = np.zeros(cap, dt)
         cnt = C.c_int64(0)
@@ -276,6 +300,11 @@ class Batch:
             return dict(H=out[:KT * KT].reshape(KT, KT), g=out[KT * KT:KT * KT + KT], d=out[KT * KT + KT:])
         if what == READ_SCALARS:
             return dict(corr=out[0], barrier=out[1], objective=out[2], face_ok=bool(out[3]))
+        if what == READ_CROP:
+            return out.copy()
+        if what == READ_FRAME_DATA:
+            return dict(xl=out[:51].copy(), yl=out[51:102].copy(), cam=out[102:106].copy(),
+                        face_size=float(out[106]), x0=int(out[107]), y0=int(out[108]))
         return out.reshape(6, -1)
 
     def render(self, want_images=True, want_tri_map=False):

@@ -8,6 +8,7 @@
 // render the next outer iteration of the reference would redo at the same point.
 #include "tdi_kernels.cu"
 #include "tdi_normal_tc.cu"
+#include "tdi_preprocess.cu"
 
 #include "../../include/tdi.h"
 
@@ -150,6 +151,9 @@ struct tdi_batch {
     size_t ne_frame_doubles = 0;   // per-frame extent of d.ne_part
     std::vector<void *> allocs;
     float *target_raw = nullptr;   // [cap][NPIX] unblurred upload
+    uint8_t *raw_stage = nullptr;  // device copies of raw video frames (tdi_batch_set_video_frames)
+    size_t raw_stage_bytes = 0;
+    PrepFrame *prep = nullptr;     // [cap] their descriptors
     float *ctrl_scratch = nullptr;
     double *scalars = nullptr;     // [cap][4]
     int *d_count = nullptr;
@@ -632,7 +636,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     int32_t *x0y0;
     tdi_status st = TDI_OK;
 #define A(ptr, n) if (st == TDI_OK) st = dalloc(b->allocs, &ptr, (n))
-    A(target, F * NPIX); A(b->target_raw, F * NPIX); A(xl, F * NL); A(yl, F * NL);
+    A(target, F * NPIX); A(b->target_raw, F * NPIX); A(b->prep, F); A(xl, F * NL); A(yl, F * NL);
     A(bounds, F * 4 * NL); A(fs, F); A(cam, F * 4); A(x0y0, F * 2); A(Lint, F);
     A(d.x, F * KTP); A(d.x_ls, F * KTP); A(d.xe, F * KTP);
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
@@ -683,18 +687,15 @@ tdi_status tdi_batch_destroy(tdi_batch *b)
         if (ln.h_count) cudaFreeHost(ln.h_count);
     }
     for (void *p : b->allocs) cudaFree(p);
+    if (b->raw_stage) cudaFree(b->raw_stage);
     if (b->h_count) cudaFreeHost(b->h_count);
     delete b;
     return TDI_OK;
 }
 
-tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *fr, void *stream)
+// Landmarks, bounds, cameras, crop origins and face sizes of a batch's frames (not the crops).
+static tdi_status set_frames_meta(tdi_batch *b, const tdi_frames *fr, cudaStream_t s)
 {
-    if (!b || !fr || !fr->targets || !fr->xl || !fr->yl || !fr->bounds || !fr->cam)
-        return fail(TDI_ERR_INVALID, "incomplete frames");
-    if (fr->n_frames <= 0) return fail(TDI_ERR_INVALID, "no frames");
-    if (fr->n_frames > b->cap) return fail(TDI_ERR_CAPACITY, "more frames than the batch holds");
-    cudaStream_t s = (cudaStream_t)stream;
     const int F = fr->n_frames;
     b->d.F = F;
     std::vector<int32_t> x0y0(2 * (size_t)F);
@@ -705,14 +706,92 @@ tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *fr, void *stream
         fs[f] = fr->face_size ? fr->face_size[f] : face_size_of(fr->xl + f * NL, fr->yl + f * NL);
     }
     DBatch &d = b->d;
-    TDI_CUDA(cudaMemcpyAsync(b->target_raw, fr->targets, sizeof(float) * NPIX * F, cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)d.xl, fr->xl, sizeof(float) * NL * F, cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)d.yl, fr->yl, sizeof(float) * NL * F, cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)d.bounds, fr->bounds, sizeof(float) * 4 * NL * F, cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)d.cam, fr->cam, sizeof(float) * 4 * F, cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)d.x0y0, x0y0.data(), sizeof(int32_t) * 2 * F, cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)d.face_size, fs.data(), sizeof(float) * F, cudaMemcpyHostToDevice, s));
-    TDI_CUDA(cudaStreamSynchronize(s));
+    TDI_CUDA(cudaStreamSynchronize(s));   // the host vectors above go out of scope
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *fr, void *stream)
+{
+    if (!b || !fr || !fr->targets || !fr->xl || !fr->yl || !fr->bounds || !fr->cam)
+        return fail(TDI_ERR_INVALID, "incomplete frames");
+    if (fr->n_frames <= 0) return fail(TDI_ERR_INVALID, "no frames");
+    if (fr->n_frames > b->cap) return fail(TDI_ERR_CAPACITY, "more frames than the batch holds");
+    cudaStream_t s = (cudaStream_t)stream;
+    TDI_CUDA(cudaMemcpyAsync(b->target_raw, fr->targets, sizeof(float) * NPIX * fr->n_frames, cudaMemcpyHostToDevice, s));
+    return set_frames_meta(b, fr, s);
+}
+
+// Raw video frames (video_fitter.cu:520-550, input_data.cu:32-53, camera.h:162-174): each
+// frame is rescaled by c = ref_face_size / face_size (float division), landmarks and camera
+// by c (float products), the crop origin and face size are taken from the rescaled
+// landmarks, and the crop is formed on the device (k_preprocess). Frames are staged on the
+// device in groups that fit PP_STAGE_BYTES.
+constexpr size_t PP_STAGE_BYTES = (size_t)256 << 20;
+
+tdi_status tdi_batch_set_video_frames(tdi_batch *b, const tdi_video_frames *fr, void *stream)
+{
+    if (!b || !fr || !fr->bgr || !fr->xp || !fr->yp || !fr->bounds || !fr->face_size || !fr->cam)
+        return fail(TDI_ERR_INVALID, "incomplete video frames");
+    if (fr->n_frames <= 0) return fail(TDI_ERR_INVALID, "no frames");
+    if (fr->n_frames > b->cap) return fail(TDI_ERR_CAPACITY, "more frames than the batch holds");
+    if (fr->width <= 0 || fr->height <= 0 || fr->row_bytes < 3 * (int64_t)fr->width)
+        return fail(TDI_ERR_INVALID, "bad image size or row pitch");
+    if (!(fr->ref_face_size > 0.0f)) return fail(TDI_ERR_INVALID, "ref_face_size must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int F = fr->n_frames;
+    std::vector<float> xl((size_t)F * NL), yl((size_t)F * NL), cam((size_t)F * 4);
+    std::vector<PrepFrame> pf(F);
+    for (int f = 0; f < F; ++f) {
+        if (!(fr->face_size[f] > 0.0f)) return fail(TDI_ERR_INVALID, "face sizes must be positive");
+        const float c = fr->ref_face_size / fr->face_size[f];
+        for (int i = 0; i < NL; ++i) {
+            xl[(size_t)f * NL + i] = c * fr->xp[(size_t)f * NL + i];
+            yl[(size_t)f * NL + i] = c * fr->yp[(size_t)f * NL + i];
+        }
+        for (int q = 0; q < 4; ++q) cam[(size_t)f * 4 + q] = fr->cam[(size_t)f * 4 + q] * c;
+        PrepFrame &p = pf[f];
+        p.row_bytes = fr->row_bytes;
+        p.width = fr->width;
+        p.height = fr->height;
+        // cv::resize: dsize = round(size * c) in double, source step 1 / c in double
+        p.rw = (int32_t)std::nearbyint((double)fr->width * (double)c);
+        p.rh = (int32_t)std::nearbyint((double)fr->height * (double)c);
+        p.inv = 1.0 / (double)c;
+        crop_origin(&xl[(size_t)f * NL], &yl[(size_t)f * NL], &p.x0, &p.y0);
+    }
+    tdi_frames tf{};
+    tf.n_frames = F;
+    tf.targets = nullptr;
+    tf.xl = xl.data();
+    tf.yl = yl.data();
+    tf.bounds = fr->bounds;
+    tf.face_size = nullptr;
+    tf.cam = cam.data();
+    tf.x0y0 = nullptr;
+    TDI_TRY(set_frames_meta(b, &tf, s));
+    const size_t fbytes = (size_t)fr->height * (size_t)fr->row_bytes;
+    const int group = (int)std::max<size_t>(1, std::min<size_t>((size_t)F, PP_STAGE_BYTES / std::max<size_t>(fbytes, 1)));
+    if (b->raw_stage_bytes < fbytes * group) {
+        TDI_CUDA(cudaStreamSynchronize(s));
+        if (b->raw_stage) { cudaFree(b->raw_stage); b->raw_stage = nullptr; b->raw_stage_bytes = 0; }
+        TDI_CUDA(cudaMalloc(&b->raw_stage, fbytes * group));
+        b->raw_stage_bytes = fbytes * group;
+    }
+    for (int f0 = 0; f0 < F; f0 += group) {
+        const int n = std::min(group, F - f0);
+        TDI_CUDA(cudaMemcpyAsync(b->raw_stage, fr->bgr + (size_t)f0 * fbytes, fbytes * n, cudaMemcpyHostToDevice, s));
+        for (int f = f0; f < f0 + n; ++f) pf[f].bgr = b->raw_stage + (size_t)(f - f0) * fbytes;
+        TDI_CUDA(cudaMemcpyAsync(b->prep + f0, pf.data() + f0, sizeof(PrepFrame) * n, cudaMemcpyHostToDevice, s));
+        TDI_TRY(launch(b, 0, k_preprocess, dim3(DIM / PP_TILE, DIM / PP_TILE, n), dim3(PP_TILE, PP_ROWS), 0, s,
+                       (const PrepFrame *)(b->prep + f0), b->target_raw + (size_t)f0 * NPIX));
+        TDI_CUDA(cudaStreamSynchronize(s));   // the stage is reused by the next group
+    }
     return TDI_OK;
 }
 
@@ -893,6 +972,26 @@ tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, 
         TDI_CUDA(cudaMemcpy(dst, b->scalars + (size_t)frame * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost));
         n = 4;
         break;
+    case 7:   // unblurred crop [NPIX], x-major
+        if (capacity < (int64_t)(NPIX * sizeof(float))) return fail(TDI_ERR_INVALID, "destination too small");
+        TDI_CUDA(cudaMemcpy(dst, b->target_raw + (size_t)frame * NPIX, NPIX * sizeof(float), cudaMemcpyDeviceToHost));
+        n = NPIX;
+        break;
+    case 8: { // frame data: xl [51], yl [51], camera [4], face size, crop origin x0, y0 (floats)
+        const int64_t cnt8 = 2 * NL + 4 + 3;
+        if (capacity < cnt8 * (int64_t)sizeof(float)) return fail(TDI_ERR_INVALID, "destination too small");
+        float *o = static_cast<float *>(dst);
+        int32_t xy[2];
+        TDI_CUDA(cudaMemcpy(o, d.xl + (size_t)frame * NL, NL * sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(o + NL, d.yl + (size_t)frame * NL, NL * sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(o + 2 * NL, d.cam + (size_t)frame * 4, 4 * sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(o + 2 * NL + 4, d.face_size + frame, sizeof(float), cudaMemcpyDeviceToHost));
+        TDI_CUDA(cudaMemcpy(xy, d.x0y0 + 2 * (size_t)frame, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        o[2 * NL + 5] = (float)xy[0];
+        o[2 * NL + 6] = (float)xy[1];
+        n = cnt8;
+        break;
+    }
     case 6: {
         if (capacity < (int64_t)(6 * (size_t)m.V * sizeof(float))) return fail(TDI_ERR_INVALID, "destination too small");
         // stored by slot; returned in the caller's vertex numbering

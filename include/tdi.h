@@ -75,6 +75,21 @@ typedef struct {
     const int32_t *x0y0;         /* [F][2] crop origins, or NULL */
 } tdi_frames;
 
+/* Frames as the reference's video fitter receives them: 8-bit BGR images at their
+ * original resolution, landmarks in original pixels, the original camera and each frame's
+ * face size (video_fitter.cu:520-550, input_data.cu:32-53, camera.h:162-174). Host arrays. */
+typedef struct {
+    int32_t n_frames;            /* F */
+    int32_t width, height;       /* size of every image */
+    int64_t row_bytes;           /* bytes from one image row to the next (>= 3 width) */
+    const uint8_t *bgr;          /* [F][height][row_bytes] B, G, R bytes per pixel */
+    const float *xp, *yp;        /* [F][51] landmarks in image pixels */
+    const float *bounds;         /* [F][4][51] lx, ly, ux, uy bound offsets in face sizes */
+    const float *face_size;      /* [F] face size in image pixels */
+    const float *cam;            /* [F][4] phix, phiy, cx, cy of the original camera */
+    float ref_face_size;         /* REF_FACE_SIZE: frames are rescaled by ref_face_size / face_size */
+} tdi_video_frames;
+
 /* Configuration keys of the reference that the path reads (config.cu:350-541). */
 typedef struct {
     int32_t max_iters_rigid;     /* outer GN iterations of the shape fit (100) */
@@ -117,6 +132,13 @@ tdi_status tdi_batch_destroy(tdi_batch *b);
 
 /* Upload frames and blur the targets (video_fitter.cu:537-550). Synchronous. */
 tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *frames, void *stream);
+/* Upload raw video frames and form their crops on the device: the reference's
+ * get_resized_frame + crop (input_data.cu:43-53, video_fitter.cu:537-550; OpenCV's
+ * BGR2GRAY, /255, INTER_LINEAR resize by ref_face_size / face_size, zero border, 256x256
+ * crop at the origin from the rescaled landmarks), its get_resized_landmarks and
+ * update_camera. Replaces tdi_batch_set_frames for callers holding decoded video frames.
+ * Synchronous. */
+tdi_status tdi_batch_set_video_frames(tdi_batch *b, const tdi_video_frames *frames, void *stream);
 /* Upload states: x [F][K+6] (epsilon, tau_x, tau_y, tau_z, u1, u2, u3), lam [F][3],
  * light intensity L [F]. Synchronous. */
 tdi_status tdi_batch_set_state(tdi_batch *b, const float *x, const float *lam, const float *L,
@@ -146,6 +168,8 @@ tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t f
  *  4 normal eq.  float [K+6][K+6] H, then [K+6] g, then [K+6] direction d
  *  5 scalars     double [4]: correlation, barrier objective, objective, face check
  *  6 geometry    float [6][V]: X0, Y0, Z0, xp, yp, camera Z
+ *  7 crop        float [65536]: the unblurred crop, x-major (after set_frames / set_video_frames)
+ *  8 frame data  float [109]: xl [51], yl [51], camera [4], face size, crop origin x0, y0
  * Returns the number of elements written through *count. Synchronous. */
 tdi_status tdi_batch_read(tdi_batch *b, int32_t frame, int32_t what, void *dst, int64_t capacity,
                           int64_t *count);
