@@ -57,7 +57,7 @@ class VideoFramesDesc(C.Structure):
     _fields_ = [("n_frames", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
                 ("row_bytes", C.c_int64), ("bgr", C.c_void_p), ("xp", C.c_void_p), ("yp", C.c_void_p),
                 ("bounds", C.c_void_p), ("face_size", C.c_void_p), ("cam", C.c_void_p),
-                ("ref_face_size", C.c_float)]
+                ("ref_face_size", C.c_float), ("ref_face_sizes", C.c_void_p)]
 
 
 class FitConfig(C.Structure):
@@ -238,8 +238,12 @@ class Batch:
         row_bytes = int(np.prod(bgr.shape[2:]))
         W = bgr.shape[2] if bgr.ndim == 4 else row_bytes // 3
         xp, yp, bounds, face_size, cam = _f32(xp), _f32(yp), _f32(bounds), _f32(face_size), _f32(cam)
+        refs = None
+        if np.ndim(ref_face_size) > 0:      # one reference size per frame
+            refs = _f32(np.broadcast_to(np.asarray(ref_face_size, np.float32), (F,)))
+            ref_face_size = 0.0
         d = VideoFramesDesc(F, W, H, row_bytes, _p(bgr), _p(xp), _p(yp), _p(bounds), _p(face_size),
-                            _p(cam), float(ref_face_size))
+                            _p(cam), float(ref_face_size), _p(refs) if refs is not None else None)
         _check(load_library().tdi_batch_set_video_frames(self.handle, C.byref(d), None))
         self.n = F
 

@@ -742,14 +742,15 @@ tdi_status tdi_batch_set_video_frames(tdi_batch *b, const tdi_video_frames *fr, 
     if (fr->n_frames > b->cap) return fail(TDI_ERR_CAPACITY, "more frames than the batch holds");
     if (fr->width <= 0 || fr->height <= 0 || fr->row_bytes < 3 * (int64_t)fr->width)
         return fail(TDI_ERR_INVALID, "bad image size or row pitch");
-    if (!(fr->ref_face_size > 0.0f)) return fail(TDI_ERR_INVALID, "ref_face_size must be positive");
+    if (!fr->ref_face_sizes && !(fr->ref_face_size > 0.0f)) return fail(TDI_ERR_INVALID, "ref_face_size must be positive");
     cudaStream_t s = (cudaStream_t)stream;
     const int F = fr->n_frames;
     std::vector<float> xl((size_t)F * NL), yl((size_t)F * NL), cam((size_t)F * 4);
     std::vector<PrepFrame> pf(F);
     for (int f = 0; f < F; ++f) {
-        if (!(fr->face_size[f] > 0.0f)) return fail(TDI_ERR_INVALID, "face sizes must be positive");
-        const float c = fr->ref_face_size / fr->face_size[f];
+        const float ref = fr->ref_face_sizes ? fr->ref_face_sizes[f] : fr->ref_face_size;
+        if (!(fr->face_size[f] > 0.0f) || !(ref > 0.0f)) return fail(TDI_ERR_INVALID, "face sizes must be positive");
+        const float c = ref / fr->face_size[f];
         for (int i = 0; i < NL; ++i) {
             xl[(size_t)f * NL + i] = c * fr->xp[(size_t)f * NL + i];
             yl[(size_t)f * NL + i] = c * fr->yp[(size_t)f * NL + i];

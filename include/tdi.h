@@ -88,6 +88,8 @@ typedef struct {
     const float *face_size;      /* [F] face size in image pixels */
     const float *cam;            /* [F][4] phix, phiy, cx, cy of the original camera */
     float ref_face_size;         /* REF_FACE_SIZE: frames are rescaled by ref_face_size / face_size */
+    const float *ref_face_sizes; /* [F] per-frame reference sizes instead (the reference's scale
+                                  * list, video_fitter.cu:271-280), or NULL */
 } tdi_video_frames;
 
 /* Configuration keys of the reference that the path reads (config.cu:350-541). */
