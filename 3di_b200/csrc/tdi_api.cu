@@ -299,7 +299,7 @@ struct Launch {
     size_t smem_vertex() const { return vt_smem(m.KP); }
     size_t smem_neigh() const { return neigh_smem(); }
     size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * NE_PD * sizeof(double); }
-    size_t smem_bar() const { return (size_t)4 * NL * m.KTP * sizeof(float); }
+    size_t smem_bar() const { return (size_t)4 * NL * NE_P8 * sizeof(float); }
     size_t smem_solve() const { return solve_smem(m.KT); }
     dim3 fblocks() const { return dim3((F + 127) / 128); }
     int A() const { return b.nact; }                      // frames active this round

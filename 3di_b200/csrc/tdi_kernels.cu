@@ -1548,21 +1548,9 @@ constexpr int NE_BPF = 32;                   // blocks per frame
 constexpr int NE_MAXCH = NMAX / NE_CH;       // chunk partials per frame at most
 static_assert(NE_THREADS == NE_CH && NE_SUB == 32 && NE_THREADS == 8 * 32, "thread mapping of the row build");
 
-// Accumulator tiles of 4 rows x 8 columns covering the upper triangle (a <= c) of a KTP x KTP
-// matrix with KTP <= 88: row block r4 (rows 4*r4..4*r4+3) needs column blocks c8 >=
-// max(0, ceil((4*r4 - 7) / 8)). NE_TILES threads own one tile each.
-constexpr int NE_TILES = 132;                // tiles for KTP = 88 (22 row blocks x up to 11 column blocks)
-
-__device__ __forceinline__ void ne_tile(int t, int &r4, int &c8)
-{
-    r4 = c8 = -1;
-    for (int r = 0; r < 22; ++r) {
-        const int c0 = max(0, (4 * r - 7 + 7) / 8);
-        const int len = 11 - c0;
-        if (t < len) { r4 = r; c8 = c0 + t; return; }
-        t -= len;
-    }
-}
+// Chunk partials are sized for the widest layout the normal-equation kernels have used:
+// 132 tiles of 4 x 8 doubles plus a row (KTP <= 88); the 8 x 8 tensor-core tiles need less.
+constexpr int NE_TILES = 132;
 
 __host__ __device__ __forceinline__ int ne_part_stride(int KTP)
 {
@@ -1827,6 +1815,23 @@ __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatc
 // Log-barrier gradient and Gauss-Newton Hessian (logbarrier_initializer.cu:1272-1843) added
 // to the image system, one block per frame.
 
+// The barrier Hessian's tensor-core updates of warp W over the 4 x 51 constraint rows (FP32
+// in shared memory, pitch NE_P8), four consecutive rows per step.
+template <int W>
+__device__ __forceinline__ void bar_hessian(double (&acc)[NE_TPW][2], const float *Fm, int KTP, int kr, int fr8)
+{
+    constexpr NeTiles TT = make_ne_tiles();
+    constexpr int NT = (NE_NT8 - W + 7) / 8;
+    for (int t = 0; t < 4 * NL; t += 4) {
+        const float *rk = Fm + (size_t)(t + kr) * KTP + fr8;
+        double v[NE_T8];
+#pragma unroll
+        for (int c = 0; c < NE_T8; ++c) v[c] = (double)rk[8 * c];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma_884(acc[j][0], acc[j][1], v[TT.bi[W + 8 * j]], v[TT.bj[W + 8 * j]]);
+    }
+}
+
 __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft_bounds)
 {
     const int f = b.act[blockIdx.x];
@@ -1835,7 +1840,7 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     if (threadIdx.x == 0) prof_count(b, KID_BARRIER);
     extern __shared__ float bsm[];
     const int KT = m.KT, KTP = m.KTP, K = m.K;
-    float *Fm = bsm;                              // [4*NL][KTP]
+    float *Fm = bsm;                              // [4*NL][NE_P8], zeros right of KT
     __shared__ float G[4][NL];
     __shared__ float s_p[NL][3];
     __shared__ float s_v[NL][3], s_ivz[NL], s_ivz2[NL];
@@ -1873,7 +1878,7 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     __syncthreads();
     // rows of the constraint gradients: warps take landmarks, lanes take columns
     for (int i = tid >> 5; i < NL; i += 8)
-    for (int a = tid & 31; a < KTP; a += 32) {
+    for (int a = tid & 31; a < NE_P8; a += 32) {
         const float p0 = s_p[i][0], p1 = s_p[i][1], p2 = s_p[i][2];
         const float vx = s_v[i][0], vy = s_v[i][1], vz = s_v[i][2];
         const float ivz = s_ivz[i], ivz2 = s_ivz2[i];
@@ -1901,10 +1906,10 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
             }
         }
         const bool live = a < KT;
-        Fm[(0 * NL + i) * KTP + a] = live ? -wx / G[0][i] : 0.0f;
-        Fm[(1 * NL + i) * KTP + a] = live ? -wy / G[1][i] : 0.0f;
-        Fm[(2 * NL + i) * KTP + a] = live ? wx / G[2][i] : 0.0f;
-        Fm[(3 * NL + i) * KTP + a] = live ? wy / G[3][i] : 0.0f;
+        Fm[(0 * NL + i) * NE_P8 + a] = live ? -wx / G[0][i] : 0.0f;
+        Fm[(1 * NL + i) * NE_P8 + a] = live ? -wy / G[1][i] : 0.0f;
+        Fm[(2 * NL + i) * NE_P8 + a] = live ? wx / G[2][i] : 0.0f;
+        Fm[(3 * NL + i) * NE_P8 + a] = live ? wy / G[3][i] : 0.0f;
     }
     __syncthreads();
     const float *lb = m.eps_b + (ft_bounds ? 2 : 0) * K;
@@ -1916,7 +1921,7 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
         const int a = tid;
         double gs = 0.0;
         for (int i = 0; i < NL; ++i)
-            for (int s = 0; s < 4; ++s) gs += (double)Fm[(s * NL + i) * KTP + a];
+            for (int s = 0; s < 4; ++s) gs += (double)Fm[(s * NL + i) * NE_P8 + a];
         float ga = (float)gs;
         if (a < K) {
             const float fub = x[a] - ub[a];
@@ -1925,37 +1930,39 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
         }
         gv[a] += ga;
     }
-    // Hessian: 4 x 8 tiles of the upper triangle (NE_TILES threads), each entry summed in FP64
-    // over the constraints in the oracle's order (set, then landmark), mirrored. The terms are
-    // products of floats, exact in FP64, so the fused multiply-add rounds like the oracle's
-    // multiply-then-add.
-    int r4, c8;
-    ne_tile(tid, r4, c8);
-    if (r4 >= 0) {
-        double acc[4][8];
+    // Hessian: H = sum over the 204 constraint rows (set, then landmark) of F_t^T F_t, each entry
+    // one FP64 fused multiply-add chain in row order, the oracle's order (the terms are
+    // products of floats, exact in FP64). On the FP64 tensor cores: mma.sync m8n8k4 adds four
+    // consecutive rows to an 8x8 tile as fma(a3, b3, fma(a2, b2, fma(a1, b1, fma(a0, b0, c)))),
+    // the same chain; 66 tiles of the upper triangle, warp W taking tiles W, W + 8, ...
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+        const int kr = lane & 3, fr8 = lane >> 2;
+        double acc[NE_TPW][2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-        for (int t = 0; t < 4 * NL; ++t) {
-            const float *row = Fm + (size_t)t * KTP;
-            const float4 a4 = *reinterpret_cast<const float4 *>(row + 4 * r4);
-            const float4 c0 = *reinterpret_cast<const float4 *>(row + 8 * c8);
-            const float4 c1 = *reinterpret_cast<const float4 *>(row + 8 * c8 + 4);
-            const double av[4] = {a4.x, a4.y, a4.z, a4.w};
-            const double cv[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], cv[j], acc[i][j]);
+        for (int j = 0; j < NE_TPW; ++j) acc[j][0] = acc[j][1] = 0.0;
+        switch (warp) {
+        case 0: bar_hessian<0>(acc, Fm, NE_P8, kr, fr8); break;
+        case 1: bar_hessian<1>(acc, Fm, NE_P8, kr, fr8); break;
+        case 2: bar_hessian<2>(acc, Fm, NE_P8, kr, fr8); break;
+        case 3: bar_hessian<3>(acc, Fm, NE_P8, kr, fr8); break;
+        case 4: bar_hessian<4>(acc, Fm, NE_P8, kr, fr8); break;
+        case 5: bar_hessian<5>(acc, Fm, NE_P8, kr, fr8); break;
+        case 6: bar_hessian<6>(acc, Fm, NE_P8, kr, fr8); break;
+        default: bar_hessian<7>(acc, Fm, NE_P8, kr, fr8); break;
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < NE_TPW; ++j) {
+            const int t = warp + 8 * j;
+            if (t >= NE_NT8) continue;
+            int bi, bj;
+            ne_tile8(t, bi, bj);
+            const int a = 8 * bi + fr8;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int a = 4 * r4 + i, c = 8 * c8 + j;
+            for (int i = 0; i < 2; ++i) {
+                const int c = 8 * bj + 2 * kr + i;
                 if (a > c || c >= KT) continue;
-                float hv = (float)acc[i][j];
+                float hv = (float)acc[j][i];
                 if (a == c && a < K) {
                     const float fub = x[a] - ub[a];
                     const float flb = lb[a] - x[a];
@@ -1966,6 +1973,7 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
                 H[(size_t)c * KTP + a] += hv;
                 if (a != c) H[(size_t)a * KTP + c] += hv;
             }
+        }
     }
 }
 
