@@ -781,25 +781,58 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
     const int e_begin = min((int)L, warp * per_e);
     const int e_end = min((int)L, e_begin + per_e);
 
-    // survivors per slot row and warp
+    // Survivors of every listed triangle, per slot row and warp. When the frame's per-warp,
+    // per-row staging fits the gradient buffer (unused until the render), the survivors are
+    // formed once here and copied to their slots after the scan; otherwise the triangles are
+    // evaluated a second time in the write pass.
+    Fragment *stage = reinterpret_cast<Fragment *>(b.fgrad + (size_t)f * 5 * NMAX);
+    const bool one_pass = (size_t)RR_WARPS * NTMP * per_e * sizeof(Fragment) <= (size_t)5 * NMAX * sizeof(float);
+    Fragment *wstage = stage + (size_t)warp * NTMP * per_e;     // [NTMP][per_e] of this warp
+    int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
+    // one listed triangle: survivor flags, owners, pixels and barycentrics of its samples
+    auto evaluate = [&](int e, bool (&sv)[NTMP], bool (&own)[NTMP], uint32_t (&pix)[NTMP],
+                        float (&al)[NTMP], float (&be)[NTMP]) -> int {
+        const int idx = __ldcg(list + e);
+        const int4 tc = __ldg(m.tl4 + idx);
+        const float4 pb = __ldg(pj + tc.x);
+        const float4 pc = __ldg(pj + tc.y);
+        const float4 pa = __ldg(pj + tc.z);
+        const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
+        const unsigned long long mykey = zkey(tag, pb.z, idx);
+        uint32_t fl2 = 0;
+        tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, fl2, [&](int r, uint32_t px, float a, float bb) {
+            const unsigned long long k = __ldcg(zb + px);
+            sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
+            own[r] = (k == mykey);
+            pix[r] = px; al[r] = a; be[r] = bb;
+        });
+        return idx;
+    };
     uint32_t cnt[NTMP] = {0, 0, 0, 0};
     for (int base = e_begin; base < e_end; base += 32) {
         const int e = base + lane;
         bool sv[NTMP] = {false, false, false, false};
-        if (e < e_end) {
-            const int idx = __ldcg(list + e);
-            const int4 tc = __ldg(m.tl4 + idx);
-            const float4 pb = __ldg(pj + tc.x);
-            const float4 pc = __ldg(pj + tc.y);
-            const float4 pa = __ldg(pj + tc.z);
-            const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
-            uint32_t fl2 = 0;
-            tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, fl2, [&](int r, uint32_t px, float, float) {
-                sv[r] = survives(__ldcg(zb + px), tag, zbits) && !(r == 0 && idx == 0);
-            });
-        }
+        bool own[NTMP] = {false, false, false, false};
+        uint32_t pix[NTMP] = {0, 0, 0, 0};
+        float al[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f}, be[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f};
+        int idx = -1;
+        if (e < e_end) idx = evaluate(e, sv, own, pix, al, be);
 #pragma unroll
-        for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
+        for (int r = 0; r < NTMP; ++r) {
+            const unsigned msk = __ballot_sync(0xffffffffu, sv[r]);
+            if (one_pass && sv[r]) {
+                Fragment fr;
+                fr.pix_owner = pix[r] | (own[r] ? 0x80000000u : 0u);
+                fr.tri = idx;
+                fr.al = al[r];
+                fr.be = be[r];
+                wstage[(size_t)r * per_e + cnt[r] + __popc(msk & lt_mask)] = fr;
+                const int px = (int)(pix[r] >> 8), py = (int)(pix[r] & 255);
+                bx0 = min(bx0, px); bx1 = max(bx1, px);
+                by0 = min(by0, py); by1 = max(by1, py);
+            }
+            cnt[r] += __popc(msk);
+        }
     }
     if (lane == 0)
         for (int r = 0; r < NTMP; ++r) s_cnt[warp][r] = cnt[r];
@@ -833,54 +866,47 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
     }
     __syncthreads();
 
-    // write survivors in slot order (row, then triangle)
-    uint32_t run[NTMP] = {0, 0, 0, 0};
+    // survivors in slot order (row, then triangle)
     uint32_t wbase[NTMP];
 #pragma unroll
     for (int r = 0; r < NTMP; ++r) wbase[r] = s_row[r] + s_off[warp][r];
     Fragment *out = b.frag + (size_t)f * NMAX;
-    int bx0 = 1 << 30, bx1 = -1, by0 = 1 << 30, by1 = -1;
-    for (int base = e_begin; base < e_end; base += 32) {
-        const int e = base + lane;
-        bool sv[NTMP] = {false, false, false, false};
-        bool own[NTMP] = {false, false, false, false};
-        uint32_t pix[NTMP] = {0, 0, 0, 0};
-        float al[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f}, be[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f};
-        int idx = -1;
-        if (e < e_end) {
-            idx = __ldcg(list + e);
-            const int4 tc = __ldg(m.tl4 + idx);
-            const float4 pb = __ldg(pj + tc.x);
-            const float4 pc = __ldg(pj + tc.y);
-            const float4 pa = __ldg(pj + tc.z);
-            const uint32_t zbits = __float_as_uint(pb.z) & 0x7FFFFFFFu;
-            const unsigned long long mykey = zkey(tag, pb.z, idx);
-            uint32_t fl2 = 0;
-            tri_samples(pb.x, pb.y, pc.x, pc.y, pa.x, pa.y, x0, y0, fl2, [&](int r, uint32_t px, float a, float bb) {
-                const unsigned long long k = __ldcg(zb + px);
-                sv[r] = survives(k, tag, zbits) && !(r == 0 && idx == 0);
-                own[r] = (k == mykey);
-                pix[r] = px; al[r] = a; be[r] = bb;
-            });
-        }
+    if (one_pass) {
 #pragma unroll
-        for (int r = 0; r < NTMP; ++r) {
-            const unsigned msk = __ballot_sync(0xffffffffu, sv[r]);
-            if (sv[r]) {
-                const uint32_t p = wbase[r] + run[r] + __popc(msk & lt_mask);
-                if (p < (uint32_t)NMAX) {
-                    Fragment fr;
-                    fr.pix_owner = pix[r] | (own[r] ? 0x80000000u : 0u);
-                    fr.tri = idx;
-                    fr.al = al[r];
-                    fr.be = be[r];
-                    out[p] = fr;
-                }
-                const int px = (int)(pix[r] >> 8), py = (int)(pix[r] & 255);
-                bx0 = min(bx0, px); bx1 = max(bx1, px);
-                by0 = min(by0, py); by1 = max(by1, py);
+        for (int r = 0; r < NTMP; ++r)
+            for (uint32_t k = lane; k < cnt[r]; k += 32) {
+                const uint32_t p = wbase[r] + k;
+                if (p < (uint32_t)NMAX) out[p] = wstage[(size_t)r * per_e + k];
             }
-            run[r] += __popc(msk);
+    } else {
+        uint32_t run[NTMP] = {0, 0, 0, 0};
+        for (int base = e_begin; base < e_end; base += 32) {
+            const int e = base + lane;
+            bool sv[NTMP] = {false, false, false, false};
+            bool own[NTMP] = {false, false, false, false};
+            uint32_t pix[NTMP] = {0, 0, 0, 0};
+            float al[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f}, be[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f};
+            int idx = -1;
+            if (e < e_end) idx = evaluate(e, sv, own, pix, al, be);
+#pragma unroll
+            for (int r = 0; r < NTMP; ++r) {
+                const unsigned msk = __ballot_sync(0xffffffffu, sv[r]);
+                if (sv[r]) {
+                    const uint32_t p = wbase[r] + run[r] + __popc(msk & lt_mask);
+                    if (p < (uint32_t)NMAX) {
+                        Fragment fr;
+                        fr.pix_owner = pix[r] | (own[r] ? 0x80000000u : 0u);
+                        fr.tri = idx;
+                        fr.al = al[r];
+                        fr.be = be[r];
+                        out[p] = fr;
+                    }
+                    const int px = (int)(pix[r] >> 8), py = (int)(pix[r] & 255);
+                    bx0 = min(bx0, px); bx1 = max(bx1, px);
+                    by0 = min(by0, py); by1 = max(by1, py);
+                }
+                run[r] += __popc(msk);
+            }
         }
     }
     if (bx1 >= 0) {
