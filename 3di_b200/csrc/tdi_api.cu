@@ -253,7 +253,7 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_barrier_full, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    TDI_CUDA(cudaFuncSetAttribute(k_precheck, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_precheck, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<NE_GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<TC_MAXN / 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     done = true;
@@ -380,7 +380,7 @@ tdi_status geometry(const Launch &L, const Cfg &c, int stage)
 {
     // the pre-render checks need only the landmarks: a rejected trial skips the vertex stage
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
-                   (size_t)PC_WARPS * (2 * L.m.K + 4 * NL + NL * PC_LM) * sizeof(float), L.s, L.m, L.b, c, stage));
+                   precheck_smem(L.m.K, L.m.KP), L.s, L.m, L.b, c, stage));
     TDI_TRY(launch(L.bt, 0, k_compact_render, dim3(1), dim3(1024), 0, L.s, L.b));
     TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, VT_WARPS + 1), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(raster_blocks(L.A()), L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));

@@ -397,32 +397,52 @@ __device__ __forceinline__ void landmark_G(const DModel &m, const DBatch &b, int
 // Both need only the 51 landmark vertices, so they run before the vertex stage: the landmark
 // object points and projections are formed here with the vertex stage's arithmetic (the same
 // values bit for bit), and a trial rejected here costs no vertex stage and no raster.
-constexpr int PC_WARPS = 4;
+constexpr int PC_WARPS = 8;                      // frames per block (a warp each)
 constexpr int PC_LM = 5;                         // per landmark: X0, Y0, Z0, xp, yp
+
+// Shared memory of k_precheck (floats): the landmarks' basis rows (pitch 3 KP + 1, staged once
+// per block for all its frames), per warp the frame's coefficients, the barrier terms and
+// the landmark points.
+__host__ __device__ __forceinline__ size_t precheck_smem(int K, int KP)
+{
+    return ((size_t)NL * (3 * KP + 1) + (size_t)PC_WARPS * (KP + 2 * K + 4 * NL + NL * PC_LM)) * sizeof(float);
+}
 
 __global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, Cfg c, int stage)
 {
-    extern __shared__ float pterm[];             // [PC_WARPS][2K + 4*NL], then [PC_WARPS][NL][PC_LM]
+    extern __shared__ float psm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int K = m.K, KP = m.KP, EP = 3 * KP + 1;
+    const int nterm = 2 * K + 4 * NL;
+    float *Es = psm;                                       // [NL][EP]
+    float *xs = Es + (size_t)NL * EP + (size_t)warp * KP;  // [KP] this warp's coefficients
+    float *pterm = Es + (size_t)NL * EP + (size_t)PC_WARPS * KP;   // [PC_WARPS][nterm]
+    float *lm = pterm + PC_WARPS * nterm + warp * NL * PC_LM;
+    // the 51 landmark basis rows, once for the block's frames
+    if (blockIdx.x * PC_WARPS >= b.nact) return;
+    for (int q = threadIdx.x; q < NL * 3 * KP; q += PC_WARPS * 32) {
+        const int li = q / (3 * KP), o = q - li * 3 * KP;
+        Es[li * EP + o] = m.E[(size_t)m.lis[li] * 3 * KP + o];
+    }
+    __syncthreads();
     const int i = blockIdx.x * PC_WARPS + warp;
     if (i >= b.nact) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active || !ctl.render) return;
-    const int nterm = 2 * m.K + 4 * NL;
-    float *lm = pterm + PC_WARPS * nterm + warp * NL * PC_LM;
     const float *x = b.xe + (size_t)f * m.KTP;
     const float *R = b.R + f * 9;
+    for (int k = lane; k < K; k += 32) xs[k] = x[k];
+    __syncwarp();
     {
-        const int K = m.K, KP = m.KP;
         const float *tau = x + K;
         const float *cam = b.cam + f * 4;
         for (int li = lane; li < NL; li += 32) {
             const int v = m.lis[li];
-            const float *er = m.E + (size_t)v * 3 * KP;
+            const float *er = Es + li * EP;
             float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
             for (int k = 0; k < K; ++k) {
-                const float xk = x[k];
+                const float xk = xs[k];
                 a0 = fmaf(er[k], xk, a0);
                 a1 = fmaf(er[KP + k], xk, a1);
                 a2 = fmaf(er[2 * KP + k], xk, a2);
