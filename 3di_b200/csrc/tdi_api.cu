@@ -304,6 +304,7 @@ struct Launch {
     dim3 fblocks() const { return dim3((F + 127) / 128); }
     int A() const { return b.nact; }                      // frames active this round
     dim3 ablocks() const { return dim3((A() + 127) / 128); }
+    dim3 wblocks() const { return dim3((A() + 3) / 4); }      // a warp per active frame, 128 threads
 };
 
 // View of frames [f0, f0 + nf) of a batch: every per-frame array starts at frame f0.
@@ -423,7 +424,7 @@ tdi_status stage_round(tdi_batch *bt, const Cfg &c, int stage, const DBatch &b, 
 {
     const DModel &m = bt->m->d;
     Launch L{bt, m, b, s, b.F};
-    TDI_TRY(launch(bt, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, b, stage));
+    TDI_TRY(launch(bt, 0, k_prepare, L.wblocks(), dim3(128), 0, s, m, b, stage));
     if (stage == ST_LAMBDA) {
         if (round == 0) {
             TDI_TRY(geometry(L, c, stage));
@@ -915,7 +916,7 @@ tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t f
     int n = 0;
     TDI_TRY(compact_active(b, s, &n));
     if (n == 0) return TDI_OK;
-    TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, stage));
+    TDI_TRY(launch(b, 0, k_prepare, L.wblocks(), dim3(128), 0, s, m, d, stage));
     TDI_TRY(geometry(L, c, stage));
     TDI_TRY(render(L, c, stage));
     TDI_TRY(launch(b, 0, k_decide_shape, L.ablocks(), dim3(128), 0, s, m, d, c, stage));
@@ -1058,7 +1059,7 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     int n = 0;
     TDI_TRY(compact_active(b, s, &n));
     if (n > 0) {
-        TDI_TRY(launch(b, 0, k_prepare, L.ablocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
+        TDI_TRY(launch(b, 0, k_prepare, L.wblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
         TDI_TRY(launch(b, 0, k_compact_render, dim3(1), dim3(1024), 0, s, (const DBatch)d));
         TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, VT_WARPS + 1), L.smem_vertex(), s, m, d));
         TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(raster_blocks(n), n), dim3(RD_THREADS), 0, s, m, d));

@@ -153,17 +153,27 @@ __global__ void k_stage_start(DModel m, DBatch b, Cfg c, int stage)
 // Evaluation point, rotation and render flag of every active frame.
 __global__ void k_prepare(DModel m, DBatch b, int stage)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // a warp per frame: the lanes copy the evaluation point, lane 0 forms R(u) and dR/du
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i >= b.nact) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
-    ctl.need_jac = 0;
-    if (!ctl.active) { ctl.render = 0; return; }
-    const float *src = (ctl.mode == M_FULL || stage == ST_LAMBDA) ? b.x : b.x_ls;
+    const bool active = ctl.active != 0;
+    const bool full = ctl.mode == M_FULL;
+    __syncwarp();
+    if (lane == 0) {
+        ctl.need_jac = 0;
+        if (!active) ctl.render = 0;
+    }
+    if (!active) return;
+    const float *src = (full || stage == ST_LAMBDA) ? b.x : b.x_ls;
     float *xe = b.xe + (size_t)f * m.KTP;
-    for (int a = 0; a < m.KT; ++a) xe[a] = src[(size_t)f * m.KTP + a];
-    rotation(xe + m.K + 3, b.R + f * 9, b.dR + f * 27);
-    ctl.render = 1;
+    for (int a = lane; a < m.KT; a += 32) xe[a] = src[(size_t)f * m.KTP + a];
+    __syncwarp();
+    if (lane == 0) {
+        rotation(xe + m.K + 3, b.R + f * 9, b.dR + f * 27);
+        ctl.render = 1;
+    }
 }
 
 // ------------------------------------------------------------------------------------------
