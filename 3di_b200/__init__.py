@@ -82,6 +82,8 @@ SIGNATURES = {
     "tdi_batch_destroy": (C.c_int32, [C.c_void_p]),
     "tdi_batch_set_frames": (C.c_int32, [C.c_void_p, C.POINTER(FramesDesc), C.c_void_p]),
     "tdi_batch_set_video_frames": (C.c_int32, [C.c_void_p, C.POINTER(VideoFramesDesc), C.c_void_p]),
+    "tdi_orthographic_init": (C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_fit": (C.c_int32, [C.c_void_p, C.POINTER(FitConfig), C.c_void_p]),
     "tdi_batch_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -189,6 +191,19 @@ class Model:
             self.close()
         except Exception:
             pass
+
+
+def orthographic_init(xl, yl, p0L):
+    """Orthographic pose initialisation of F frames (tdi_orthographic_init): landmarks xl, yl
+    [F][51], the model's landmark points p0L [3][51]. Returns x [F][7] (tau_x, tau_y,
+    sigma_x, sigma_y, u1, u2, u3), yaw/pitch/roll in degrees [F][3] and iterations [F]."""
+    xl, yl, p0L = _f32(xl), _f32(yl), _f32(p0L)
+    F = xl.shape[0]
+    x = np.zeros((F, 7), np.float32)
+    ypr = np.zeros((F, 3), np.float32)
+    it = np.zeros(F, np.int32)
+    _check(load_library().tdi_orthographic_init(F, _p(xl), _p(yl), _p(p0L), _p(x), _p(ypr), _p(it), None))
+    return x, ypr, it
 
 
 class Batch:

@@ -9,10 +9,12 @@
 #include "tdi_kernels.cu"
 #include "tdi_normal_tc.cu"
 #include "tdi_preprocess.cu"
+#include "tdi_orthographic.cu"
 
 #include "../../include/tdi.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -923,6 +925,64 @@ tdi_status tdi_batch_evaluate(tdi_batch *b, const tdi_fit_config *cfg, int32_t f
     TDI_TRY(normal_equations(L, c, stage));
     TDI_TRY(launch(b, 0, k_scalars, L.fblocks(), dim3(128), 0, s, d, b->scalars));
     TDI_CUDA(cudaStreamSynchronize(s));
+    return TDI_OK;
+}
+
+// Euler angles in degrees of a column-major rotation (rotation_header.cu:421-449, RAD2DEG of
+// constants.h:59): atan2 in double, rounded to float.
+static void euler_degrees(const float *R, float *ypr)
+{
+    const float c = std::sqrt(R[5] * R[5] + R[8] * R[8]);
+    float yaw, pitch, roll;
+    if (!(c < 1e-6f)) {
+        roll = (float)std::atan2((double)R[1], (double)R[0]);
+        yaw = (float)std::atan2((double)-R[2], (double)c);
+        pitch = (float)std::atan2((double)R[5], (double)R[8]);
+    } else {
+        roll = (float)std::atan2((double)-R[7], (double)R[4]);
+        yaw = (float)std::atan2((double)-R[2], (double)c);
+        pitch = 0.0f;
+    }
+    ypr[0] = (float)((double)(yaw * 180.0f) / M_PI);
+    ypr[1] = (float)((double)(pitch * 180.0f) / M_PI);
+    ypr[2] = (float)((double)(roll * 180.0f) / M_PI);
+}
+
+tdi_status tdi_orthographic_init(int32_t n_frames, const float *xl, const float *yl, const float *p0L,
+                                 float *x_out, float *ypr_out, int32_t *iters_out, void *stream)
+{
+    if (n_frames <= 0 || !xl || !yl || !p0L || !x_out) return fail(TDI_ERR_INVALID, "bad orthographic arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t F = (size_t)n_frames;
+    const size_t nf = 2 * F * NL + 3 * NL + F * OR_N + F * 9;
+    float *dbuf = nullptr;
+    int32_t *dit = nullptr;
+    TDI_CUDA(cudaMalloc(&dbuf, nf * sizeof(float)));
+    if (cudaMalloc(&dit, F * sizeof(int32_t)) != cudaSuccess) { cudaFree(dbuf); return fail(TDI_ERR_CUDA, "cudaMalloc"); }
+    float *dxl = dbuf, *dyl = dxl + F * NL, *dp = dyl + F * NL, *dx = dp + 3 * NL, *dR = dx + F * OR_N;
+    std::vector<float> R(F * 9);
+    std::vector<int32_t> it(F);
+    tdi_status st = TDI_OK;
+    auto run = [&]() -> tdi_status {
+        TDI_CUDA(cudaMemcpyAsync(dxl, xl, F * NL * sizeof(float), cudaMemcpyHostToDevice, s));
+        TDI_CUDA(cudaMemcpyAsync(dyl, yl, F * NL * sizeof(float), cudaMemcpyHostToDevice, s));
+        TDI_CUDA(cudaMemcpyAsync(dp, p0L, 3 * NL * sizeof(float), cudaMemcpyHostToDevice, s));
+        k_orthographic<<<(unsigned)((F + OR_WARPS - 1) / OR_WARPS), OR_WARPS * 32, 0, s>>>(dxl, dyl, dp, n_frames, dx, dR, dit);
+        TDI_CUDA(cudaGetLastError());
+        TDI_CUDA(cudaMemcpyAsync(x_out, dx, F * OR_N * sizeof(float), cudaMemcpyDeviceToHost, s));
+        TDI_CUDA(cudaMemcpyAsync(R.data(), dR, F * 9 * sizeof(float), cudaMemcpyDeviceToHost, s));
+        TDI_CUDA(cudaMemcpyAsync(it.data(), dit, F * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        TDI_CUDA(cudaStreamSynchronize(s));
+        return TDI_OK;
+    };
+    st = run();
+    cudaFree(dbuf);
+    cudaFree(dit);
+    if (st != TDI_OK) return st;
+    for (size_t f = 0; f < F; ++f) {
+        if (ypr_out) euler_degrees(&R[f * 9], ypr_out + f * 3);
+        if (iters_out) iters_out[f] = it[f];
+    }
     return TDI_OK;
 }
 

@@ -92,6 +92,16 @@ typedef struct {
                                   * list, video_fitter.cu:271-280), or NULL */
 } tdi_video_frames;
 
+/* Orthographic pose initialisation of many frames (OrthographicInitializer::fit_model,
+ * orthographic_initializer.cu:243-380): per frame a 7-parameter Gauss-Newton fit
+ * x = (tau_x, tau_y, sigma_x, sigma_y, u1, u2, u3) of the scaled orthographic projection of
+ * the model's landmark points p0L [3][51] (p0L_mat.dat) to the frame's centred landmarks
+ * xl, yl [F][51], from the reference's start point. Outputs x [F][7], the yaw, pitch and roll
+ * in degrees of the last trial rotation [F][3] (or NULL) and the outer iterations [F]
+ * (or NULL). Host arrays; allocates its device buffers; synchronous. */
+tdi_status tdi_orthographic_init(int32_t n_frames, const float *xl, const float *yl, const float *p0L,
+                                 float *x_out, float *ypr_out, int32_t *iters_out, void *stream);
+
 /* Configuration keys of the reference that the path reads (config.cu:350-541). */
 typedef struct {
     int32_t max_iters_rigid;     /* outer GN iterations of the shape fit (100) */

@@ -209,6 +209,15 @@ def rotation(u, kind="f32"):
     return R, dR.reshape(3, 9)
 
 
+def orthographic(xl, yl, p0L, kind="f32"):
+    """Orthographic pose initialisation of one frame: (x [7], rotation of the last trial [9],
+    outer iterations)."""
+    x = np.zeros(7, np.float32)
+    R = np.zeros(9, np.float32)
+    q = lib(kind).o_orthographic_f(_p(_f32(xl)), _p(_f32(yl)), _p(_f32(p0L)), _p(x), _p(R))
+    return x, R, q
+
+
 def vertex_stage(model: Model, x, cam, ref_face_size=78.0, kind="f32"):
     geo = np.zeros((8, model.V), np.float32)
     ok = lib(kind).o_vertex_stage_f(C.byref(model.s), _p(_f32(x)), _p(_f32(cam)),

@@ -1182,3 +1182,103 @@ int o_render_image_f(const o_model *m, const o_frame *f, const o_config *cfg, co
     ctx_free(&c);
     return N;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* OrthographicInitializer::fit_model (orthographic_initializer.cu:243-380) for one frame:
+ * a Gauss-Newton fit of x = (tau_x, tau_y, sigma_x, sigma_y, u1, u2, u3) so that the scaled
+ * orthographic projection (sigma_x (R p + tau)_x, sigma_y (R p + tau)_y) of the model's
+ * landmark points p (p0L, [3][51]) meets the centred landmarks, from the reference's start
+ * point (0, 0, 15, 15, 0, 0, 0.05) (:152-167), Armijo line search with alpha 0.4 and beta 0.5
+ * down to t = 0.1, at most 100 outer iterations. FP32 as the reference; its library calls in
+ * a fixed order: landmark means as sequential float sums (thrust::reduce), R p as
+ * ((R0 p0 + R3 p1) + R6 p2) (cublasSgemm), J^T J, J^T e and the dot products as float fused
+ * multiply-add chains over the 102 residual rows in order (x rows, then y rows), the 7 x 7
+ * system with solve(). Writes x and the rotation of the last trial point (the one the
+ * reference's Euler angles are read from, :366-373). Returns the outer iterations run. */
+#define ORTH_N 7
+#define ORTH_ROWS (2 * O_NL)
+
+static void orth_rp(const float *R, const float *p0L, int i, float *r)
+{
+    const float p0 = p0L[i], p1 = p0L[O_NL + i], p2 = p0L[2 * O_NL + i];
+    for (int k = 0; k < 3; ++k) r[k] = (R[k] * p0 + R[3 + k] * p1) + R[6 + k] * p2;
+}
+
+int o_orthographic_f(const float *xl, const float *yl, const float *p0L, float *x, float *R_last)
+{
+    float xb[O_NL], yb[O_NL], xm = 0.0f, ym = 0.0f;
+    for (int i = 0; i < O_NL; ++i) { xm += xl[i]; ym += yl[i]; }
+    xm = xm / (float)O_NL;
+    ym = ym / (float)O_NL;
+    for (int i = 0; i < O_NL; ++i) { xb[i] = xl[i] - xm; yb[i] = yl[i] - ym; }
+    const float x0[ORTH_N] = {0.0f, 0.0f, 15.0f, 15.0f, 0.0f, 0.0f, 0.05f};
+    for (int n = 0; n < ORTH_N; ++n) x[n] = x0[n];
+    for (int k = 0; k < 9; ++k) R_last[k] = 0.0f;
+    int terminate = 0, q;
+    for (q = 0; q < 100; ++q) {
+        if (terminate) break;
+        float R[9], dR[27];
+        o_rotation_f(x + 4, R, dR);
+        float W[ORTH_N][ORTH_ROWS];
+        float e[ORTH_ROWS];
+        for (int i = 0; i < O_NL; ++i) {
+            float rp[3], d[3][3];
+            orth_rp(R, p0L, i, rp);
+            for (int a = 0; a < 3; ++a) orth_rp(dR + 9 * a, p0L, i, d[a]);
+            W[0][i] = x[2];        W[0][O_NL + i] = 0.0f;
+            W[1][i] = 0.0f;        W[1][O_NL + i] = x[3];
+            W[2][i] = x[0] + rp[0]; W[2][O_NL + i] = 0.0f;
+            W[3][i] = 0.0f;        W[3][O_NL + i] = x[1] + rp[1];
+            for (int a = 0; a < 3; ++a) {
+                W[4 + a][i] = x[2] * d[a][0];
+                W[4 + a][O_NL + i] = x[3] * d[a][1];
+            }
+            e[i] = x[2] * (rp[0] + x[0]) - xb[i];
+            e[O_NL + i] = x[3] * (rp[1] + x[1]) - yb[i];
+        }
+        float JTJ[ORTH_N * ORTH_N], dg[ORTH_N], obj = 0.0f, sd[ORTH_N];
+        for (int a = 0; a < ORTH_N; ++a)
+            for (int b = 0; b < ORTH_N; ++b) {
+                float s = 0.0f;
+                for (int r = 0; r < ORTH_ROWS; ++r) s = fmaf(W[a][r], W[b][r], s);
+                JTJ[b * ORTH_N + a] = s;
+            }
+        for (int a = 0; a < ORTH_N; ++a) {
+            float s = 0.0f;
+            for (int r = 0; r < ORTH_ROWS; ++r) s = fmaf(W[a][r], e[r], s);
+            dg[a] = s;
+        }
+        for (int r = 0; r < ORTH_ROWS; ++r) obj = fmaf(e[r], e[r], obj);
+        {
+            real Hr[ORTH_N * ORTH_N], gr[ORTH_N], dr[ORTH_N];   /* exact copies in either build */
+            for (int k = 0; k < ORTH_N * ORTH_N; ++k) Hr[k] = JTJ[k];
+            for (int k = 0; k < ORTH_N; ++k) gr[k] = dg[k];
+            solve(Hr, gr, ORTH_N, dr);
+            for (int k = 0; k < ORTH_N; ++k) sd[k] = (float)dr[k];
+        }
+        float t = 1.0f;
+        for (int inner = 0; inner < 1000; ++inner) {
+            if (t < 0.1f) { terminate = 1; break; }
+            float xs[ORTH_N], Rt[9], dRt[27];
+            for (int n = 0; n < ORTH_N; ++n) xs[n] = x[n] + t * sd[n];
+            o_rotation_f(xs + 4, Rt, dRt);
+            for (int k = 0; k < 9; ++k) R_last[k] = Rt[k];
+            float et[ORTH_ROWS], objt = 0.0f, tmp = 0.0f;
+            for (int i = 0; i < O_NL; ++i) {
+                float rp[3];
+                orth_rp(Rt, p0L, i, rp);
+                et[i] = xs[2] * (rp[0] + xs[0]) - xb[i];
+                et[O_NL + i] = xs[3] * (rp[1] + xs[1]) - yb[i];
+            }
+            for (int r = 0; r < ORTH_ROWS; ++r) objt = fmaf(et[r], et[r], objt);
+            for (int n = 0; n < ORTH_N; ++n) tmp = fmaf(sd[n], dg[n], tmp);
+            tmp *= 0.4f * t;
+            if (objt < obj + tmp) {
+                for (int n = 0; n < ORTH_N; ++n) x[n] = xs[n];
+                break;
+            }
+            t = t * 0.5f;
+        }
+    }
+    return q;
+}
