@@ -1574,18 +1574,6 @@ __global__ void __launch_bounds__(JAC_THREADS, 4) k_jacobian(DModel m, DBatch b)
     }
 }
 
-// Chain rule through the normalised gradient (newfuncs.cu:417-463) of fragment n, column j.
-__device__ __forceinline__ void chain(const float *Jf, int ld, const int32_t *nb, int n, int j,
-                                      float gx, float gy, float pre, float &ox, float &oy)
-{
-    const float dh = Jf[(size_t)nb[1 * NMAX + n] * ld + j] - Jf[(size_t)nb[0 * NMAX + n] * ld + j];
-    const float dv = Jf[(size_t)nb[3 * NMAX + n] * ld + j] - Jf[(size_t)nb[2 * NMAX + n] * ld + j];
-    const float diffx = 2 * gx, diffy = 2 * gy;
-    const float X = (-diffy) * (-dh) - (-diffx) * (-dv);
-    ox = ((-pre) * (-diffy)) * X;
-    oy = (pre * (-diffx)) * X;
-}
-
 // ------------------------------------------------------------------------------------------
 // Normal equations of the image term (derivative_computer.cu:135-164): rows of
 // d(gx/|g|)/dtheta and d(gy/|g|)/dtheta, H = tau * sum(row row^T), g = -tau * sum(w row).
