@@ -197,7 +197,9 @@ def fit_multiscale(batch, bgr, xp, yp, bounds, face_size, cam, x0, lam0, L, cfg,
         a = np.asarray(a, F32)
         return a.reshape(S * T, a.shape[2]) if a.ndim == 3 else np.concatenate([a] * S)
 
-    rep_ = lambda a: np.concatenate([np.asarray(a)] * S)
+    def rep_(a):               # the same frames for every scale
+        return np.concatenate([np.asarray(a)] * S)
+
     refs = np.repeat(np.asarray(sizes, F32), T)
     batch.set_video_frames(rep_(bgr), rep_(xp), rep_(yp), rep_(bounds), rep_(face_size), rep_(cam), refs)
     x0s, lam0s, Ls = per_scale(x0), per_scale(lam0), rep_(np.asarray(L, F32))
