@@ -30,6 +30,7 @@ FLAG_STUCK_NEG_TZ = 8
 FLAG_CHOL_FAILED = 16
 FLAG_FAIL = 32
 FLAG_OVERFLOW = 64
+FLAG_BAD_INDEX = 128
 
 READ_FRAGMENTS, READ_NEIGHBOURS, READ_GRADIENTS, READ_JACOBIAN, READ_NORMAL_EQ, READ_SCALARS, \
     READ_GEOMETRY, READ_CROP, READ_FRAME_DATA = range(9)

@@ -6,8 +6,15 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libtdi_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "tdi_api.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("tdi_kernels.cu", "tdi_internal.cuh", "tdi_noalloc.cu", "tdi_normal_tc.cu", "tdi_async.cuh")] + [
-    os.path.join(HERE, "..", "include", "tdi.h")]
+
+
+def deps() -> list:
+    """Every source the library is built from: tdi_api.cu includes the other csrc files."""
+    csrc = os.path.join(HERE, "csrc")
+    return sorted(os.path.join(csrc, f) for f in os.listdir(csrc) if f.endswith((".cu", ".cuh", ".h"))) + [
+        os.path.join(HERE, "..", "include", "tdi.h")]
+
+
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
     # formulas are restated operation by operation: no FMA contraction, IEEE div/sqrt
@@ -27,7 +34,7 @@ def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(p) <= t for p in DEPS)
+    return all(os.path.getmtime(p) <= t for p in deps())
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:

@@ -34,6 +34,7 @@ constexpr uint32_t FLAG_STUCK_NEG_TZ = 8u;
 constexpr uint32_t FLAG_CHOL_FAILED = 16u;
 constexpr uint32_t FLAG_FAIL = 32u;
 constexpr uint32_t FLAG_OVERFLOW = 64u;       // more fragments than NMAX
+constexpr uint32_t FLAG_BAD_INDEX = 128u;     // a triangle corner outside the vertex arrays (skipped)
 
 enum Stage : int32_t { ST_LAMBDA = 0, ST_RIGID = 1, ST_FINETUNE = 2 };
 enum Mode : int32_t { M_IDLE = 0, M_FULL = 1, M_TRIAL = 2 };

@@ -16,9 +16,13 @@
 //    nothing carries over between calls, but two calls whose kernels overlap on the GPU
 //    (different streams, or different host threads) race on the array and give undefined
 //    fragments. Serialise calls on one stream.
-//  * the first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//    with that device current; make that first call before any stream capture begins.
-#include <mutex>
+//  * the triangle corners are caller-owned device memory that the host cannot check: a
+//    triangle with a corner outside [0, n_vertices) is skipped on the device before any
+//    vertex is read and the call's flags get TDI_FLAG_BAD_INDEX;
+//  * every call looks up the array's device address (cudaGetSymbolAddress, which allocates
+//    nothing) with the caller's device current, so a device reset between calls is safe. The
+//    first call on a device also loads the library's device code there; make that first call
+//    before any stream capture begins.
 
 namespace tdi {
 
@@ -37,7 +41,7 @@ static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 // slot order, same owner rule, with the scratch above and the caller's output arrays (16-byte records: pixel | owner<<31,
 // triangle, float bits of alpha and beta).
 __global__ void __cluster_dims__(NA_RC, 1, 1) __launch_bounds__(1024)
-k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_t *tl, int T,
+k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_t *tl, int V, int T,
                  int x0, int y0, NoAllocScratch *scr, int32_t *frags, int capacity,
                  int32_t *count, uint32_t *flags_out)
 {
@@ -75,8 +79,14 @@ k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_
     for (int base = t_begin; base < t_end; base += 32) {
         const int idx = base + lane;
         if (idx < t_end) {
+            // corners outside the vertex arrays: the triangle has no fragments and no vertex
+            // is read; the passes below skip it through its zero count
+            const bool ok = (uint32_t)tl[idx] < (uint32_t)V && (uint32_t)tl[T + idx] < (uint32_t)V &&
+                            (uint32_t)tl[2 * T + idx] < (uint32_t)V;
             uint16_t pix[NTMP]; float al[NTMP], be[NTMP];
-            const int nf = tri_fragments(dm, xp, yp, idx, x0, y0, pix, al, be, flags);
+            int nf = 0;
+            if (ok) nf = tri_fragments(dm, xp, yp, idx, x0, y0, pix, al, be, flags);
+            else flags |= FLAG_BAD_INDEX;
             cnt8[idx] = (uint8_t)nf;
             if (nf) {
                 const float Z = zc[tl[idx]];
@@ -198,14 +208,6 @@ k_raster_noalloc(const float *xp, const float *yp, const float *zc, const int32_
 
 }  // namespace tdi
 
-namespace {
-
-std::mutex g_noalloc_mu;
-constexpr int NOALLOC_MAX_DEVICES = 256;
-tdi::NoAllocScratch *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
-
-}  // namespace
-
 extern "C" tdi_status tdi_raster_noalloc(const float *xp, const float *yp, const float *zc,
                                          const int32_t *triangles, int32_t n_vertices,
                                          int32_t n_triangles, int32_t x0, int32_t y0,
@@ -219,23 +221,14 @@ extern "C" tdi_status tdi_raster_noalloc(const float *xp, const float *yp, const
         return fail(TDI_ERR_INVALID, "tdi_raster_noalloc: sizes must be positive");
     if (n_triangles > NOALLOC_MAX_TRIANGLES)
         return fail(TDI_ERR_CAPACITY, "tdi_raster_noalloc: at most 131072 triangles (fixed working array)");
-    int dev = 0;
-    TDI_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(TDI_ERR_INVALID, "tdi_raster_noalloc: device ordinal");
+    // The array's name is only a host-side stand-in: the kernel needs its address on the
+    // current device, looked up on every call (no allocation; valid after a device reset).
     NoAllocScratch *scr = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess)
-                return fail(TDI_ERR_CUDA, std::string("tdi_raster_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = static_cast<NoAllocScratch *>(p);
-        }
-        scr = g_noalloc_ptr[dev];
-    }
-    k_raster_noalloc<<<NA_RC, 1024, 0, (cudaStream_t)stream>>>(xp, yp, zc, triangles, n_triangles, x0, y0,
-                                                            scr, fragments, capacity, count, flags);
+    cudaError_t e0 = cudaGetSymbolAddress((void **)&scr, g_noalloc_scratch);
+    if (e0 != cudaSuccess)
+        return fail(TDI_ERR_CUDA, std::string("tdi_raster_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e0));
+    k_raster_noalloc<<<NA_RC, 1024, 0, (cudaStream_t)stream>>>(xp, yp, zc, triangles, n_vertices, n_triangles,
+                                                            x0, y0, scr, fragments, capacity, count, flags);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(TDI_ERR_CUDA, std::string("tdi_raster_noalloc: launch: ") + cudaGetErrorString(e));
     return TDI_OK;

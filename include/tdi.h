@@ -40,7 +40,9 @@ typedef int32_t tdi_status;
 #define TDI_FLAG_STUCK_NEG_TZ 8u     /* a trial with tau_z < 0 (model_fitter.cu:255-259) */
 #define TDI_FLAG_CHOL_FAILED 16u     /* Cholesky factorisation failed (solver.h:87-92) */
 #define TDI_FLAG_FAIL 32u            /* outer iterations <= NITERS_SUCCESS (model_fitter.cu:374) */
-#define TDI_FLAG_OVERFLOW 64u        /* more than 32,768 fragments */
+#define TDI_FLAG_OVERFLOW 64u        /* more than 32,768 fragments (tdi_raster_noalloc: more than capacity) */
+#define TDI_FLAG_BAD_INDEX 128u      /* tdi_raster_noalloc: a triangle corner outside [0, n_vertices);
+                                        that triangle is skipped */
 
 typedef struct tdi_model tdi_model;
 typedef struct tdi_batch tdi_batch;
@@ -217,12 +219,15 @@ tdi_status tdi_batch_profile_read(tdi_batch *b, int64_t *launches, double *total
  * for the same projections: device arrays xp, yp, camera Z [n_vertices], triangles
  * [3][n_triangles] (0-based), crop origin; output: fragments int32 [capacity][4] (pixel |
  * owner<<31, triangle, float bits of alpha, beta) in slot order, *count (device int32, the
- * number written) and *flags (device uint32, TDI_FLAG_*). Calls no allocator: its working
+ * number written, at most capacity; TDI_FLAG_OVERFLOW when more survived) and *flags (device
+ * uint32, TDI_FLAG_*). A triangle with a corner outside [0, n_vertices) is skipped on the
+ * device before any vertex is read (TDI_FLAG_BAD_INDEX). Calls no allocator: its working
  * memory is a fixed 640 KiB array in the library's device image, held on every device that
  * loads the library until the process exits. At most 131,072 triangles (TDI_ERR_CAPACITY
  * otherwise). Calls share that array: calls that overlap on the GPU race; serialise them on
- * one stream. The first call on a device looks the array up (cudaGetSymbolAddress) with that
- * device current, so make it before any stream capture. Asynchronous on the stream. */
+ * one stream. Every call looks the array up (cudaGetSymbolAddress, no allocation) with the
+ * caller's device current; the first call on a device also loads the library's device code
+ * there, so make it before any stream capture. Asynchronous on the stream. */
 tdi_status tdi_raster_noalloc(const float *xp, const float *yp, const float *zc,
                               const int32_t *triangles, int32_t n_vertices, int32_t n_triangles,
                               int32_t x0, int32_t y0, int32_t *fragments, int32_t capacity,
