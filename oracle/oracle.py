@@ -40,7 +40,7 @@ class OConfig(C.Structure):
     _fields_ = [("max_iters_rigid", C.c_int32), ("max_iters_finetune", C.c_int32),
                 ("twostage_illum", C.c_int32), ("finetune", C.c_int32),
                 ("niters_success", C.c_int32), ("max_iters_lambda", C.c_int32),
-                ("ref_face_size", C.c_float), ("taps", C.c_float * 15)]
+                ("ref_face_size", C.c_float), ("taps", C.c_float * 15), ("damping", C.c_float)]
 
 
 class OReport(C.Structure):
@@ -64,6 +64,7 @@ def lib(kind: str = "f32") -> C.CDLL:
         L.o_raster_f.restype = C.c_int
         L.o_render_image_f.restype = C.c_int
         L.o_vertex_stage_f.restype = C.c_int
+        L.o_image_terms_f.restype = C.c_int
         L.o_max_threads.restype = C.c_int
         _LIBS[kind] = L
     return _LIBS[kind]
@@ -114,7 +115,7 @@ class FrameSet:
 
 
 def config(max_iters_rigid=100, max_iters_finetune=100, twostage_illum=0, finetune=0,
-           niters_success=6, max_iters_lambda=10000, ref_face_size=78.0, taps=None) -> OConfig:
+           niters_success=6, max_iters_lambda=10000, ref_face_size=78.0, taps=None, damping=0.0) -> OConfig:
     if taps is None:
         import importlib.util
         spec = importlib.util.spec_from_file_location(
@@ -124,6 +125,7 @@ def config(max_iters_rigid=100, max_iters_finetune=100, twostage_illum=0, finetu
         taps = mod.KERNEL_SIGMA_TAPS[0.75]
     c = OConfig(max_iters_rigid, max_iters_finetune, twostage_illum, finetune, niters_success,
                 max_iters_lambda, ref_face_size)
+    c.damping = float(damping)
     for i, t in enumerate(taps):
         c.taps[i] = t
     return c
@@ -171,6 +173,19 @@ def evaluate(model: Model, frames: FrameSet, j: int, cfg: OConfig, x, lam, L,
                corr=o["scal"][0], barrier=o["scal"][1], objective=o["scal"][2],
                face_ok=bool(o["scal"][3]))
     return out
+
+
+def image_terms(model: Model, frames: FrameSet, j: int, cfg: OConfig, x, lam, L, tau_img=25.0,
+                kind="f32") -> dict:
+    """Normal equations of the image term alone (no barrier terms) and the correlation sum."""
+    KT = model.K + 6
+    H = np.zeros((KT, KT), np.float32)
+    g = np.zeros(KT, np.float32)
+    corr = C.c_double(0)
+    N = lib(kind).o_image_terms_f(C.byref(model.s), C.byref(frames.arr[j]), C.byref(cfg), _p(_f32(x)),
+                                  _p(_f32(lam)), C.c_float(float(L)), C.c_float(float(tau_img)), _p(H), _p(g),
+                                  C.byref(corr))
+    return dict(N=N, H=H, g=g, corr=corr.value)
 
 
 def raster(model: Model, xp, yp, Z, x0, y0, kind="f32") -> dict:

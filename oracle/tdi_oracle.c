@@ -647,11 +647,13 @@ static double barrier(const o_model *m, const o_frame *f, const real *x, const r
 /* ------------------------------------------------------------------------------------ */
 /* Solver::solve (solver.h:70-105): FP64 Cholesky of H (lower triangle), x = H^-1 g,
  * direction d = -x. Returns 0 and NaN directions when the factorisation fails. */
-static int solve(const real *H, const real *g, int n, real *d)
+static int solve(const real *H, const real *g, int n, real *d, float damping)
 {
     double *L = (double *)malloc(sizeof(double) * n * n);
     double *y = (double *)malloc(sizeof(double) * n);
     for (int i = 0; i < n * n; ++i) L[i] = (double)H[i];
+    /* damped solve (H + lambda I) x = g, lambda added in double; 0 = the reference's solve */
+    for (int i = 0; i < n; ++i) L[i * n + i] += (double)damping;
     int ok = 1;
     for (int j = 0; j < n && ok; ++j) {
         double s = L[j * n + j];
@@ -893,7 +895,7 @@ static void fit_lambdas(ctx_t *c, const real *x, real *lam, real Lint)
         real H[9], gv[3], d[3];
         for (int i = 0; i < 9; ++i) H[i] = (real)Hs[i];
         for (int i = 0; i < 3; ++i) gv[i] = (real)(-gs[i]);
-        solve(H, gv, 3, d);
+        solve(H, gv, 3, d, 0.0f);
         {
             real l2n = (real)((double)d[0] * gv[0] + (double)d[1] * gv[1] + (double)d[2] * gv[2]);
             if (isnan((double)l2n)) break;    /* every trial would be rejected down to t < 0.01 */
@@ -944,7 +946,7 @@ static int fit_shape(ctx_t *c, real *x, real *x_ls, const real *lam, real Lint, 
         image_normal_equations(c, tau_img, H, gv);
         double ob = barrier(m, c->f, x, c->R, c->dR, finetune, H, gv);
         grad_corr = grad_corr + (-(real)ob);
-        if (!solve(H, gv, KT, d)) c->rep->flags |= O_FLAG_CHOL_FAILED;
+        if (!solve(H, gv, KT, d, c->cfg->damping)) c->rep->flags |= O_FLAG_CHOL_FAILED;
         if (isnan((double)d[0])) { c->rep->flags |= O_FLAG_NAN_DIRECTION; terminate = 1; break; }
         real t = 1.0f;
         const real ALPHA = 0.4f, BETA = 0.8f;
@@ -1138,7 +1140,7 @@ int o_evaluate_f(const o_model *m, const o_frame *f, const o_config *cfg, const 
     const real tau_img = (real)25.0f;
     image_normal_equations(&c, tau_img, Hr, gr);
     double ob = barrier(m, f, xr, c.R, c.dR, finetune_bounds, Hr, gr);
-    if (!solve(Hr, gr, KT, dr)) rep.flags |= O_FLAG_CHOL_FAILED;
+    if (!solve(Hr, gr, KT, dr, cfg->damping)) rep.flags |= O_FLAG_CHOL_FAILED;
     real grad_corr = tau_img * (real)corr;
     grad_corr = grad_corr + (-(real)ob);
     if (slot) memcpy(slot, c.fr.slot, sizeof(int32_t) * N);
@@ -1159,6 +1161,35 @@ int o_evaluate_f(const o_model *m, const o_frame *f, const o_config *cfg, const 
     if (scal) { scal[0] = corr; scal[1] = ob; scal[2] = (double)(-grad_corr); scal[3] = face_ok; }
     if (flags) *flags = rep.flags;
     free(Hr); free(gr); free(dr);
+    ctx_free(&c);
+    return N;
+}
+
+/* The image term alone at a state: H = tau (Gx^T Gx + Gy^T Gy) and g = -tau (gxs^T Gx +
+ * gys^T Gy) (derivative_computer.cu:135-164) without the barrier terms, and the correlation
+ * sum; what the reference's DerivativeComputer forms before Logbarrier_Initializer adds its
+ * part. Returns N. */
+int o_image_terms_f(const o_model *m, const o_frame *f, const o_config *cfg, const float *x,
+                    const float *lam, float Lint, float tau_img, float *H, float *g, double *corr)
+{
+    o_report rep;
+    memset(&rep, 0, sizeof(rep));
+    ctx_t c;
+    ctx_init(&c, m, f, cfg, &rep);
+    const int KT = m->K + 6;
+    real xr[512], lr[3] = {lam[0], lam[1], lam[2]};
+    for (int a = 0; a < KT; ++a) xr[a] = x[a];
+    geometry_and_raster(&c, xr, 1);
+    const int N = c.fr.n;
+    double cs = image_term(&c, xr, lr, (real)Lint);
+    const size_t nkt = (size_t)(KT > 0 ? KT : 1);
+    real *Hr = (real *)calloc(nkt * nkt, sizeof(real));
+    real *gr = (real *)calloc(nkt, sizeof(real));
+    image_normal_equations(&c, (real)tau_img, Hr, gr);
+    for (int i = 0; i < KT * KT; ++i) H[i] = (float)Hr[i];
+    for (int i = 0; i < KT; ++i) g[i] = (float)gr[i];
+    if (corr) *corr = cs;
+    free(Hr); free(gr);
     ctx_free(&c);
     return N;
 }
@@ -1253,7 +1284,7 @@ int o_orthographic_f(const float *xl, const float *yl, const float *p0L, float *
             real Hr[ORTH_N * ORTH_N], gr[ORTH_N], dr[ORTH_N];   /* exact copies in either build */
             for (int k = 0; k < ORTH_N * ORTH_N; ++k) Hr[k] = JTJ[k];
             for (int k = 0; k < ORTH_N; ++k) gr[k] = dg[k];
-            solve(Hr, gr, ORTH_N, dr);
+            solve(Hr, gr, ORTH_N, dr, 0.0f);
             for (int k = 0; k < ORTH_N; ++k) sd[k] = (float)dr[k];
         }
         float t = 1.0f;

@@ -61,6 +61,7 @@ typedef struct {
     int32_t max_iters_lambda;    /* outer iterations of fit_3DMM_lambdas (10000) */
     float ref_face_size;         /* REF_FACE_SIZE */
     float taps[O_NTAPS];         /* Gaussian blur taps */
+    float damping;               /* lambda of the damped shape solve (H + lambda I); 0 = undamped */
 } o_config;
 
 /* frame status bits */
