@@ -102,6 +102,7 @@ __global__ void k_scalars(DBatch b, double *out)   // [F][4]
 tdi_status check_cfg(const tdi_fit_config &c, const DModel &m)
 {
     if (c.normal_eq != 0 && c.normal_eq != 1) return fail(TDI_ERR_INVALID, "normal_eq must be 0 or 1");
+    if (!(c.damping >= 0.0f) || !(c.damping < 3.0e38f)) return fail(TDI_ERR_INVALID, "damping must be finite and >= 0");
     if (c.normal_eq == 1 && m.KT + 1 > TC_MAXN)
         return fail(TDI_ERR_INVALID, "tensor-core normal equations take at most 121 expression components");
     if (c.normal_eq == 0 && m.KT + 1 > NE_P8)
@@ -121,6 +122,7 @@ Cfg to_cfg(const tdi_fit_config &c)
     r.ref_face_size = c.ref_face_size;
     for (int i = 0; i < NTAPS; ++i) r.taps[i] = c.taps[i];
     r.normal_eq = c.normal_eq;
+    r.damping = c.damping;
     return r;
 }
 

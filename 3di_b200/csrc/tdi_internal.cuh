@@ -76,6 +76,7 @@ struct Cfg {
     float ref_face_size;
     float taps[NTAPS];
     int32_t normal_eq;       // 0: FP64 in the oracle's order; 1: split-BF16 tensor cores
+    float damping;           // lambda of the damped shape solve (H + lambda I), 0 = undamped
 };
 
 // Device view of the model.

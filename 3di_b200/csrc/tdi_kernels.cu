@@ -2059,12 +2059,14 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
     const float *H = b.H + (size_t)f * KTP * KTP;
     const float *gv = b.g + (size_t)f * KTP;
     double v[RB][RB];
+    const double lam_d = (double)c.damping;      // damped solve: H + lambda I (0: undamped)
 #pragma unroll
     for (int a = 0; a < RB; ++a)
 #pragma unroll
         for (int bb = 0; bb < RB; ++bb) {
             const int i = tr + 16 * a, l = tc + 16 * bb;
             v[a][bb] = (i < n && l < n && i >= l) ? (double)H[(size_t)l * KTP + i] : 0.0;
+            if (i == l && i < n) v[a][bb] += lam_d;
         }
     double y = tid < n ? (double)gv[tid] : 0.0;
     if (tid == 0) piv[1] = 0.0;

@@ -48,8 +48,6 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=1024, help="frames per GPU per step")
     ap.add_argument("--cpu-frames", type=int, default=8, help="frames of the CPU sample")
-    ap.add_argument("--profile-kernel", default="vertex",
-                    help="kernel timed live for the roofline (the largest share of the step)")
     ap.add_argument("--plain-frames", type=int, default=16, help="frames of the unbatched (plain) run")
     ap.add_argument("--normal-eq", default="exact", choices=["exact", "tensor"],
                     help="normal equations: FP64 in the oracle's order, or split-BF16 on the tensor cores")
@@ -143,8 +141,15 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+KERNELS = ["vertex", "raster", "raster_resolve", "render", "neighbours", "jacobian", "normal_eq", "barrier",
+           "solve"]
+FP64_NOMINAL_TFLOPS = 40.0   # B200 FP64 tensor, nominal (no measured FP64 figure on this pool)
+
+
 def algorithmic_bytes(kernel: str, V: int, T: int, K: int, n_frag: float):
-    """(bytes per frame, bytes per launch) a kernel must move: what the roofline divides by."""
+    """(bytes per frame, bytes per launch) a kernel must move: what the roofline divides by.
+    None for the latency-bound per-frame kernels (barrier terms, Cholesky)."""
+    KT = K + 6
     if kernel == "vertex":
         # outputs per frame (object coordinates 12 B, projection x, y, Z 12 B per vertex) and
         # the coefficients; the basis (3*V*K*4 B) once per launch, shared by all its frames.
@@ -155,13 +160,29 @@ def algorithmic_bytes(kernel: str, V: int, T: int, K: int, n_frag: float):
         # depth pass: projections (16 B per vertex), triangle corners and visiting order
         # (16 B per triangle), one 8-byte depth key per visible fragment
         return 16.0 * V + 16.0 * T + 8.0 * n_frag, 0.0
+    if kernel == "raster_resolve":
+        # the frame's triangle mask, the corners and projections of the triangles with
+        # fragments (about one per fragment), their depth keys and the fragment records written
+        return T / 8.0 + n_frag * (16 + 3 * 16 + 8 + 16), 0.0
     if kernel == "render":
         # fragments, three vertices' object coordinates and albedo, four target pixels, gradients
         return n_frag * (16 + 3 * 16 + 4 * 4 + 5 * 4), 0.0
+    if kernel == "neighbours":
+        # fragment pixels in, four neighbour indices out
+        return n_frag * (16 + 16), 0.0
     if kernel == "jacobian":
         # three vertices' basis rows (3 coords x K) and the row written
-        return n_frag * (3 * 3 * K * 4 + (K + 6) * 4), 0.0
-    raise ValueError(kernel)
+        return n_frag * (3 * 3 * K * 4 + KT * 4), 0.0
+    if kernel == "normal_eq":
+        # every Jacobian row read once, gradients and neighbour indices, the chunk partials
+        return n_frag * (KT * 4 + 5 * 4 + 16) + 128 * KT * KT * 8 / 2, 0.0
+    return None, None
+
+
+def normal_eq_flops_per_frame(K: int, n_frag: float) -> float:
+    """Algorithmic flops of J^T J and J^T r: 2 (2N) K^2 + 2 (2N) K (the x and y rows)."""
+    KT = K + 6
+    return 2.0 * 2 * n_frag * KT * KT + 2.0 * 2 * n_frag * KT
 
 
 def vertex_flops_per_frame(V: int, K: int) -> float:
@@ -222,6 +243,88 @@ def render_targets_cpu(O, synth, m, fr):
     fr.target = synth.add_noise(np.stack(imgs), 0.02, 3)
 
 
+def fit_timed(batch, cfg, fr, lam0, L, steps, barrier):
+    """Device time (ms) of `steps` fits of the resident batch, each from the initial states."""
+    import torch
+    total = 0.0
+    for _ in range(steps):
+        batch.set_state(fr.state_init, lam0, L)      # reset the fitted states (not timed)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.fit(cfg)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        total += e0.elapsed_time(e1)
+    return total
+
+
+def kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl):
+    """Every major kernel timed live with CUDA events on its stream, one untimed fit per kernel
+    (tdi_batch_profile): launches, device time, frames processed, share of the kernels' sum,
+    and its roofline against its algorithmic bytes (or flops)."""
+    rows = {}
+    for name in KERNELS:
+        batch.set_state(fr.state_init, lam0, L)
+        batch.profile(name)
+        batch.fit(cfg)
+        n, ms, frames = batch.profile_read()
+        batch.profile(None)
+        rows[name] = {"launches": n, "ms": ms, "frames": frames}
+    total = sum(r["ms"] for r in rows.values())
+    for name, r in rows.items():
+        r["share"] = r["ms"] / total if total else None
+        r["us_per_frame"] = 1000.0 * r["ms"] / r["frames"] if r["frames"] else None
+        per_frame, per_launch = algorithmic_bytes(name, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
+        if per_frame is not None and r["launches"]:
+            avg_s = r["ms"] / 1000.0 / r["launches"]
+            fpl = r["frames"] / r["launches"]
+            bpl = per_frame * fpl + per_launch
+            r["hbm_gbs"] = bpl / avg_s / 1e9
+            r["hbm_frac"] = r["hbm_gbs"] / hbm
+        if name == "normal_eq" and r["launches"]:
+            fl = normal_eq_flops_per_frame(m.n_expr, n_frag) * r["frames"] / (r["ms"] / 1000.0) / 1e12
+            r["tflops"] = fl
+            r["tflops_frac_of_peak"] = fl / (tfl if cfg.normal_eq == 1 else FP64_NOMINAL_TFLOPS)
+            r["tflops_peak"] = "measured bf16" if cfg.normal_eq == 1 else "nominal FP64 tensor (40 TFLOP/s)"
+        if name == "vertex" and r["launches"]:
+            r["fp32_tflops"] = vertex_flops_per_frame(m.n_vertices, m.n_expr) * r["frames"] / (r["ms"] / 1000.0) / 1e12
+            r["fp32_frac_of_nominal"] = r["fp32_tflops"] / FP32_NOMINAL_TFLOPS
+    return rows
+
+
+def step_error_table(O, om, fs, fr, lam0, L, tdi, batch, n, cfg):
+    """Errors of every output of one Gauss-Newton step against the FP64 oracle, from the same
+    state (the frames' initial states), by parameter group: H blocks (relative Frobenius), g,
+    d and the first trial point x + d (relative max norm), the objective (relative)."""
+    K = om.K
+    groups = {"expr": slice(0, K), "pose": slice(K, K + 6)}
+    batch.set_state(fr.state_init, lam0, L)
+    batch.evaluate(cfg)
+    acc = {}
+    for i in range(n):
+        x = fr.state_init[i]
+        e = O.evaluate(om, fs, i, O.config(), x, lam0[i], float(L[i]), kind="f64")
+        ne = batch.read(i, tdi.READ_NORMAL_EQ)
+        sc = batch.read(i, tdi.READ_SCALARS)
+        H, Ho = ne["H"].astype(np.float64), e["H"].astype(np.float64)
+        r = {}
+        for a, sa in groups.items():
+            for b, sb in groups.items():
+                r[f"H_{a}_{b}"] = np.linalg.norm(H[sa, sb] - Ho[sa, sb]) / np.linalg.norm(Ho[sa, sb])
+        for a, sa in groups.items():
+            for name, v, vo in (("g", ne["g"], e["g"]), ("d", ne["d"], e["d"]), ("trial", x + ne["d"], x + e["d"])):
+                vo = vo.astype(np.float64)
+                r[f"{name}_{a}"] = np.abs(v[sa] - vo[sa]).max() / max(np.abs(vo[sa]).max(), 1e-30)
+        r["objective"] = abs(sc["objective"] - e["objective"]) / abs(e["objective"])
+        for k, v in r.items():
+            acc.setdefault(k, []).append(float(v))
+    return {k: {"median": float(np.median(v)), "max": float(np.max(v))} for k, v in acc.items()}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -251,8 +354,8 @@ def main():
     fr.target = synth.add_noise(img, 0.02, 3 + rank)
     batch.set_frames(fr)
     lam0 = np.tile(synth.LAMBDA_INIT, (F, 1)).astype(np.float32)
-    cfg = tdi.default_config(max_iters_rigid=MAX_ITERS,
-                             normal_eq=tdi.NORMAL_EQ_TENSOR if args.normal_eq == "tensor" else tdi.NORMAL_EQ_EXACT)
+    neq = tdi.NORMAL_EQ_TENSOR if args.normal_eq == "tensor" else tdi.NORMAL_EQ_EXACT
+    cfg = tdi.default_config(max_iters_rigid=MAX_ITERS, normal_eq=neq)
 
     def barrier():
         if world > 1:
@@ -267,27 +370,14 @@ def main():
     # timed: device-resident inputs
     clocks = ClockSampler(local)
     clocks.start()
-    batch.profile(args.profile_kernel)
     launches0 = batch.launches()
-    total_ms = 0.0
-    for _ in range(args.steps):
-        batch.set_state(fr.state_init, lam0, L)      # reset the fitted states (not timed)
-        barrier()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        batch.fit(cfg)
-        e1.record()
-        torch.cuda.synchronize()
-        barrier()
-        total_ms += e0.elapsed_time(e1)
+    total_ms = fit_timed(batch, cfg, fr, lam0, L, args.steps, barrier)
     launches = batch.launches() - launches0
-    prof_launches, prof_ms, prof_frames = batch.profile_read()
-    batch.profile(None)
     clk = clocks.stop()
     x, lamf, rep = batch.get_state()
     n_frag = float(np.mean([r.n_fragments for r in rep]))
+    gn_iters = int(sum(r.iters_rigid + r.iters_finetune for r in rep))
+    renders = int(sum(r.renders for r in rep))
 
     # timed: end to end from pinned host memory through tdi_fit_frames
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
@@ -321,42 +411,38 @@ def main():
                                normal_eq=tdi.NORMAL_EQ_TENSOR if other == "tensor" else tdi.NORMAL_EQ_EXACT)
     batch.set_state(fr.state_init, lam0, L)
     batch.fit(cfg_o)
-    other_ms = 0.0
-    for _ in range(args.steps):
-        batch.set_state(fr.state_init, lam0, L)
-        barrier()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        batch.fit(cfg_o)
-        e1.record()
-        torch.cuda.synchronize()
-        barrier()
-        other_ms += e0.elapsed_time(e1)
+    other_ms = fit_timed(batch, cfg_o, fr, lam0, L, args.steps, barrier)
     xo_gpu, _, rep_o = batch.get_state()
+    # the reference's cfg1 stage sequence: two-stage illumination and the expression finetune
+    cfg1 = tdi.default_config(max_iters_rigid=MAX_ITERS, max_iters_finetune=MAX_ITERS, twostage_illum=1,
+                              finetune=1, normal_eq=neq)
+    batch.set_state(fr.state_init, lam0, L)
+    batch.fit(cfg1)
+    cfg1_ms = fit_timed(batch, cfg1, fr, lam0, L, args.steps, barrier)
+    _, _, rep1 = batch.get_state()
     h2d = sum(h[k].numel() * h[k].element_size() for k in ("t", "xl", "yl", "b", "fs", "cam", "o", "x", "lam", "L"))
     d2h = F * (m.n_expr + 6) * 4 + F * 3 * 4 + F * C.sizeof(tdi.Report)
 
     # max over ranks
-    total_ms, e2e_ms, other_ms = max_over_ranks([total_ms, e2e_ms, other_ms], world, device="cuda")
+    total_ms, e2e_ms, other_ms, cfg1_ms = max_over_ranks([total_ms, e2e_ms, other_ms, cfg1_ms], world, device="cuda")
     frames_all = F * world * args.steps
     value = job_rate(F, world, args.steps, total_ms)
     e2e = job_rate(F, world, args.steps, e2e_ms)
 
+    # per-kernel live timing (untimed fits) and the roofline of the largest-share kernel
     hbm, tfl, peak_kind = measured_peaks()
-    per_frame, per_launch = algorithmic_bytes(args.profile_kernel, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
-    avg_launch_s = prof_ms / 1000.0 / max(prof_launches, 1)
-    frames_per_launch = prof_frames / max(prof_launches, 1)
-    bytes_per_launch = per_frame * frames_per_launch + per_launch
-    achieved = bytes_per_launch / avg_launch_s / 1e9 if prof_launches else None
+    kt = kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl)
+    top = max((k for k in kt if "hbm_gbs" in kt[k]), key=lambda k: kt[k]["ms"])
+    per_frame, per_launch = algorithmic_bytes(top, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
+    tr_ = kt[top]
+    fpl = tr_["frames"] / max(tr_["launches"], 1)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            tr = json.load(f).get(args.profile_kernel)
+            tr = json.load(f).get(top)
         if tr:
-            traffic = tr["dram_bytes_per_frame"] * frames_per_launch + tr.get("dram_bytes_per_launch", 0.0)
+            traffic = tr["dram_bytes_per_frame"] * fpl + tr.get("dram_bytes_per_launch", 0.0)
 
     line = {
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
@@ -373,26 +459,26 @@ def main():
         "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": args.profile_kernel, "bound": "hbm", "achieved": achieved,
-                     "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm if achieved else None, "traffic": traffic,
-                     "peak_source": peak_kind, "launches": prof_launches,
-                     "avg_launch_ms": avg_launch_s * 1000.0, "frames_per_launch": frames_per_launch,
+        "gn_iters_per_s": gn_iters * world * args.steps / (total_ms / 1000.0),
+        "evaluations_per_s": renders * world * args.steps / (total_ms / 1000.0),
+        "roofline": {"kernel": top, "bound": "hbm", "achieved": tr_["hbm_gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": tr_["hbm_frac"], "traffic": traffic, "peak_source": peak_kind,
+                     "share": tr_["share"], "launches": tr_["launches"],
+                     "avg_launch_ms": tr_["ms"] / max(tr_["launches"], 1), "frames_per_launch": fpl,
                      "algorithmic_bytes_per_frame": per_frame, "algorithmic_bytes_per_launch": per_launch},
-        "compute": ({"kernel": "vertex", "achieved": vertex_flops_per_frame(m.n_vertices, m.n_expr) * frames_per_launch
-                                                     / avg_launch_s / 1e12,
-                     "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-                     "frac": vertex_flops_per_frame(m.n_vertices, m.n_expr) * frames_per_launch / avg_launch_s / 1e12
-                             / FP32_NOMINAL_TFLOPS,
-                     "peak_source": "nominal FP32 SIMT: 148 SMs x 128 lanes x 2 flops x 1.965 GHz",
-                     "note": "basis x coefficients as a sequential FP32 FMA chain (bit-exact order), no tensor-core form"}
-                    if args.profile_kernel == "vertex" and prof_launches else None),
+        "kernels": kt,
         "normal_eq_modes": {args.normal_eq: {"value": value, "ms_per_step": total_ms / args.steps},
                             other: {"value": frames_all / (other_ms / 1000.0), "ms_per_step": other_ms / args.steps,
                                     "mean_renders": float(np.mean([r.renders for r in rep_o])),
                                     "failed": int(sum(1 for r in rep_o if r.flags & tdi.FLAG_FAIL))},
                             "note": "exact: FP64 normal equations in the oracle's order (bit-identical fits); "
                                     "tensor: split-BF16 tcgen05 products, FP32 chunk accumulation"},
+        "stage_sequences": {"light_shape": {"value": value, "note": "light fit + shape fit (one face scale)"},
+                            "cfg1": {"value": frames_all / (cfg1_ms / 1000.0), "ms_per_step": cfg1_ms / args.steps,
+                                     "mean_iters_finetune": float(np.mean([r.iters_finetune for r in rep1])),
+                                     "note": "light, shape, two-stage illumination (2 more light + shape fits) "
+                                             "and the expression finetune, as the reference's cfg1 runs each "
+                                             "face scale"}},
         "clocks": clk,
         "fit": {"mean_iters_rigid": float(np.mean([r.iters_rigid for r in rep])),
                 "mean_iters_lambda": float(np.mean([r.iters_lambda for r in rep])),
@@ -422,6 +508,7 @@ def main():
             line["batched_over_plain"] = value / line["plain"]["value"]
 
         if args.cpu_frames > 0:
+            # CPU baseline leg: the oracle timed on the host cores, then used as the checker
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import oracle as O
             O.build()
@@ -438,12 +525,26 @@ def main():
             for kind in ("f32", "f64"):
                 ox, ol, orep = O.fit_frames(om, fs, ocfg, fr.state_init[:n], lam0[:n], L[:n], kind=kind)
                 for mode, xg in ((args.normal_eq, x), (other, xo_gpu)):
+                    key = "vs_" + ("fp32" if kind == "f32" else "fp64") + "_oracle"
                     rel = np.abs(xg[:n] - ox) / np.maximum(np.abs(ox), 1e-2)
-                    errs[mode]["vs_" + ("fp32" if kind == "f32" else "fp64") + "_oracle"] = {
+                    K = m.n_expr
+                    errs[mode][key] = {
                         "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+                        "pose_median_rel": float(np.median(rel[:, K:])), "pose_max_rel": float(rel[:, K:].max()),
                         "frames_within_1e-5": int(np.sum(rel.max(axis=1) <= 1e-5))}
+                    if mode == args.normal_eq:
+                        errs[mode][key]["light_max_rel"] = float(
+                            (np.abs(lamf[:n] - ol) / np.maximum(np.abs(ol), 1e-6)).max())
             line["param_err"] = {"frames": n, **errs[args.normal_eq], other: errs[other],
-                                 "definition": "|x_gpu - x_oracle| / max(|x_oracle|, 1e-2) over pose and expressions"}
+                                 "definition": "|x_gpu - x_oracle| / max(|x_oracle|, 1e-2) over pose and expressions "
+                                               "after the whole fit; light: |lam_gpu - lam_oracle| / |lam_oracle|"}
+            # every output of one Gauss-Newton step against the FP64 oracle, both modes
+            line["step_err"] = {
+                "frames": n,
+                args.normal_eq: step_error_table(O, om, fs, fr, lam0, L, tdi, batch, n, cfg),
+                other: step_error_table(O, om, fs, fr, lam0, L, tdi, batch, n, cfg_o),
+                "definition": "one evaluation at the initial states vs the FP64 oracle: H blocks relative "
+                              "Frobenius, g, d and x + d relative max norm per group, objective relative"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     batch.close()

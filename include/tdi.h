@@ -120,6 +120,10 @@ typedef struct {
                                   *     accumulation per 256-fragment chunk (g stays exact).
                                   *     No counterpart in the reference (which uses
                                   *     cublasSgemm). */
+    float damping;               /* lambda of the shape solve's damped Cholesky: the Gauss-Newton
+                                  * system (H + lambda I) d = -g, lambda >= 0 added in FP64 to the
+                                  * diagonal before the factorisation. 0 = the reference's undamped
+                                  * solve (Solver::solve, solver.h:70-105). */
 } tdi_fit_config;
 
 typedef struct {

@@ -1,0 +1,129 @@
+"""The reference's full per-frame stage sequence on the GPU, and the error of every output of
+one Gauss-Newton step against the FP64 oracle.
+
+cfg1 stage sequence (video_fitter.cu:560-648, model_fitter.cu:397-672): light fit, shape fit,
+two more light/shape rounds (TWOSTAGE_ILLUM) and the expression finetune with widened bounds
+and the line search's stale pose (FINETUNE_EXPRESSIONS). The product must follow the FP32
+oracle's iterates exactly: same flags, same iteration counts, states within 1e-5.
+
+Per-step error table: from one state, the normal equations H and g, the search direction d,
+the first trial point x + d and the objective, each split into the expression and pose
+groups, for both normal-equation modes against the FP64 oracle (the same arithmetic in
+double). The bounds are stated in STEP_BOUNDS."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# Stated per-step bounds against the FP64 oracle (relative: Frobenius for H blocks, max norm
+# for vectors and for the objective). Measured on B200 over 8 frames of the 53,490-vertex video
+# workload (maxima): exact mode H 1.7e-5, g 1.5e-4, d pose 8.1e-3, x + d pose 4.8e-4, objective
+# 1.2e-5; tensor mode H 1.7e-5, g 1.6e-4, d pose 0.17, x + d pose 9.6e-3. The exact mode is the
+# reference's FP32 arithmetic, so these are the reference's own distances from FP64: the
+# search direction inherits the conditioning of H (poorly determined expression components).
+STEP_BOUNDS = {
+    "exact": {"H": 1e-4, "g": 1e-3, "objective": 1e-4, "d_pose": 5e-2, "trial_pose": 5e-3},
+    "tensor": {"H": 1e-4, "g": 1e-3, "objective": 1e-4, "d_pose": 0.5, "trial_pose": 5e-2},
+}
+
+
+def _setup(tdi, case, synth):
+    tdi.require_gpu()
+    m, fr, om = case
+    model = tdi.Model(m)
+    batch = tdi.Batch(model, fr.n_frames)
+    batch.set_frames(fr)
+    lam = np.tile(synth.LAMBDA_INIT, (fr.n_frames, 1))
+    L = np.full(fr.n_frames, synth.L_INTENSITY, np.float32)
+    return model, batch, lam, L
+
+
+@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+def test_cfg1_stage_sequence_matches_oracle(request, tdi, synth, O, case_name):
+    """Light, shape, two-stage illumination and expression finetune, as cfg1 runs them."""
+    case = request.getfixturevalue(case_name)
+    m, fr, om = case
+    model, batch, lam, L = _setup(tdi, case, synth)
+    kw = dict(max_iters_rigid=10, max_iters_finetune=10, twostage_illum=1, finetune=1)
+    x, lamf, rep = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(**kw))
+    ox, olam, orep = O.fit_frames(om, O.FrameSet(fr), O.config(**kw), fr.state_init, lam, L)
+    for i in range(fr.n_frames):
+        assert rep[i].flags == orep[i].flags, i
+        assert rep[i].iters_rigid == orep[i].iters_rigid, i
+        assert rep[i].iters_finetune == orep[i].iters_finetune, i
+        assert rep[i].iters_lambda == orep[i].iters_lambda, i
+        assert rep[i].iters_finetune > 0
+        err = np.abs(x[i] - ox[i]) / np.maximum(np.abs(ox[i]), 1e-2)
+        assert err.max() <= 1e-5, err.max()
+        np.testing.assert_allclose(lamf[i], olam[i], rtol=1e-5, atol=1e-7)
+
+
+def step_errors(tdi, batch, O, om, fs, fr, lam, L, mode):
+    """Per-group relative errors of one evaluation (H, g, d, x + d, objective) against the FP64
+    oracle, for every frame of the batch; the batch has been evaluated at fr.state_init."""
+    K = om.K
+    groups = {"expr": slice(0, K), "pose": slice(K, K + 6)}
+    rows = []
+    for i in range(fs.n):
+        x = fr.state_init[i]
+        e = O.evaluate(om, fs, i, O.config(), x, lam[i], float(L[i]), kind="f64")
+        ne = batch.read(i, tdi.READ_NORMAL_EQ)
+        sc = batch.read(i, tdi.READ_SCALARS)
+        H, Ho = ne["H"].astype(np.float64), e["H"].astype(np.float64)
+        r = {}
+        for a, sa in groups.items():
+            for b, sb in groups.items():
+                r[f"H_{a}_{b}"] = float(np.linalg.norm(H[sa, sb] - Ho[sa, sb]) / np.linalg.norm(Ho[sa, sb]))
+        for a, sa in groups.items():
+            for name, v, vo in (("g", ne["g"], e["g"]), ("d", ne["d"], e["d"]),
+                                ("trial", x + ne["d"], x + e["d"])):
+                vo = vo.astype(np.float64)
+                r[f"{name}_{a}"] = float(np.abs(v[sa] - vo[sa]).max() / max(np.abs(vo[sa]).max(), 1e-30))
+        r["objective"] = float(abs(sc["objective"] - e["objective"]) / abs(e["objective"]))
+        rows.append(r)
+    return rows
+
+
+@pytest.mark.parametrize("mode", ["exact", "tensor"])
+@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+def test_step_errors_against_fp64_oracle(request, tdi, synth, O, case_name, mode):
+    case = request.getfixturevalue(case_name)
+    m, fr, om = case
+    model, batch, lam, L = _setup(tdi, case, synth)
+    batch.set_state(fr.state_init, lam, L)
+    batch.evaluate(tdi.default_config(normal_eq=tdi.NORMAL_EQ_TENSOR if mode == "tensor" else tdi.NORMAL_EQ_EXACT))
+    rows = step_errors(tdi, batch, O, om, O.FrameSet(fr), fr, lam, L, mode)
+    b = STEP_BOUNDS[mode]
+    for i, r in enumerate(rows):
+        print(f"{case_name} {mode} frame {i}: " + ", ".join(f"{k} {v:.1e}" for k, v in r.items()))
+        for k in ("H_expr_expr", "H_pose_pose", "H_expr_pose"):
+            assert r[k] <= b["H"], (k, r[k])
+        assert r["g_expr"] <= b["g"] and r["g_pose"] <= b["g"]
+        assert r["objective"] <= b["objective"]
+        assert r["d_pose"] <= b["d_pose"]
+        assert r["trial_pose"] <= b["trial_pose"]
+
+
+def test_damped_solve_matches_oracle(tdi, synth, O, small_case):
+    """Damped Cholesky (H + lambda I) d = -g in the shape solve (the survey's R14 option; the
+    reference's Solver::solve is undamped, lambda = 0): the damped fit follows the oracle's
+    damped iterates, and the damped direction differs from the undamped one."""
+    m, fr, om = small_case
+    model, batch, lam, L = _setup(tdi, small_case, synth)
+    damp = 1e3
+    batch.set_state(fr.state_init, lam, L)
+    batch.evaluate(tdi.default_config(damping=damp))
+    fs = O.FrameSet(fr)
+    for i in range(fr.n_frames):
+        e = O.evaluate(om, fs, i, O.config(damping=damp), fr.state_init[i], lam[i], float(L[i]))
+        e0 = O.evaluate(om, fs, i, O.config(), fr.state_init[i], lam[i], float(L[i]))
+        ne = batch.read(i, tdi.READ_NORMAL_EQ)
+        assert np.linalg.norm(ne["d"] - e["d"]) <= 1e-4 * np.linalg.norm(e["d"])
+        assert np.linalg.norm(e["d"] - e0["d"]) > 1e-3 * np.linalg.norm(e0["d"])
+    cfg = dict(max_iters_rigid=10, damping=damp)
+    x, lamf, rep = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(**cfg))
+    ox, olam, orep = O.fit_frames(om, fs, O.config(**cfg), fr.state_init, lam, L)
+    for i in range(fr.n_frames):
+        assert rep[i].flags == orep[i].flags and rep[i].iters_rigid == orep[i].iters_rigid
+        err = np.abs(x[i] - ox[i]) / np.maximum(np.abs(ox[i]), 1e-2)
+        assert err.max() <= 1e-5, err.max()

@@ -223,3 +223,19 @@ def test_fit_is_deterministic_and_descends(O, small_case, synth):
         e0 = O.evaluate(om, fs, i, cfg, fr.state_init[i], l1[i], synth.L_INTENSITY)
         assert r1[i].objective <= e0["objective"] + 1e-3 * abs(e0["objective"])
         assert r1[i].iters_rigid >= 1 and r1[i].iters_lambda >= 1
+
+
+def test_damped_direction_solves_the_shifted_system(synth, O, small_case):
+    """The oracle's damped solve: d solves (H + lambda I) d = -g for the H and g it returns;
+    lambda = 0 is the undamped solve."""
+    m, fr, om = small_case
+    lam = synth.LAMBDA_INIT
+    L = float(synth.L_INTENSITY)
+    fs = O.FrameSet(fr)
+    e0 = O.evaluate(om, fs, 0, O.config(), fr.state_init[0], lam, L)
+    for damp in (0.0, 1e3):
+        e = O.evaluate(om, fs, 0, O.config(damping=damp), fr.state_init[0], lam, L)
+        H = e["H"].astype(np.float64) + damp * np.eye(len(e["g"]))
+        r = H @ e["d"].astype(np.float64) + e["g"].astype(np.float64)
+        assert np.linalg.norm(r) <= 1e-4 * np.linalg.norm(e["g"])
+    assert np.array_equal(O.evaluate(om, fs, 0, O.config(damping=0.0), fr.state_init[0], lam, L)["d"], e0["d"])
