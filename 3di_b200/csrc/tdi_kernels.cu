@@ -190,6 +190,18 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 // vertex-tile stripes, so that every block has work whatever share of the active frames
 // the pre-render checks rejected.
 
+// Two IEEE fused multiply-adds in one instruction (sm_100 packed FP32): d.x = fma(a.x, b.x, c.x),
+// d.y = fma(a.y, b.y, c.y), round to nearest, denormals kept -- the same results as two fmaf.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c)
+{
+    float2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(reinterpret_cast<unsigned long long &>(d))
+        : "l"(reinterpret_cast<const unsigned long long &>(a)), "l"(reinterpret_cast<const unsigned long long &>(b)),
+          "l"(reinterpret_cast<const unsigned long long &>(c)));
+    return d;
+}
+
 constexpr int VT_V = 32;                                   // vertices per tile (one per lane)
 constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
 constexpr int VT_FR = 16;                                   // per-frame floats: R(9), tau(3), cam(4)
@@ -208,7 +220,7 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
     extern __shared__ __align__(16) float vsm[];
     const int KP = m.KP, K = m.K, ER = vt_row(KP);
     float *Eb = vsm;                           // [2][VT_V][ER]: basis rows of two tiles
-    float *Xs = Eb + 2 * VT_V * ER;            // [VT_F][KP]: coefficients per frame
+    float *Xs = Eb + 2 * VT_V * ER;            // [KP][VT_F]: coefficients, the block's frames innermost
     float *Fs = Xs + VT_F * KP;                // [VT_F][VT_FR]
     __shared__ int s_any;
     __shared__ volatile int s_abort;
@@ -253,7 +265,7 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
         for (int fl = threadIdx.y; fl < VT_F; fl += VT_WARPS) {
             const int f = s_frame[fl];
             const float *xr = f >= 0 ? b.xe + (size_t)f * m.KTP : nullptr;
-            for (int k = threadIdx.x; k < KP; k += 32) Xs[fl * KP + k] = (xr && k < K) ? xr[k] : 0.0f;
+            for (int k = threadIdx.x; k < KP; k += 32) Xs[k * VT_F + fl] = (xr && k < K) ? xr[k] : 0.0f;
             if (threadIdx.x < VT_FR) {
                 const int i = threadIdx.x;
                 float v = 0.0f;
@@ -299,7 +311,7 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
         }
     } else {
         const int vl = threadIdx.x;
-        const float *xr = Xs + (threadIdx.y * VT_FPT) * KP;
+        const float *xr = Xs + threadIdx.y * VT_FPT;      // this warp's 8 frames at k: xr[k * VT_F + q]
         for (int j = 0;; ++j) {
             const int t = gy + j * groups;
             if (t >= ntiles) break;
@@ -314,10 +326,12 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
                 break;
             }
             const float *er = Eb + (size_t)(buf * VT_V + vl) * ER;
-            float acc[VT_FPT][3];
+            // Sequential fused multiply-add over k for every output (the order the oracle uses),
+            // two frames per instruction: each half of fma.rn.f32x2 is an IEEE fused
+            // multiply-add, so every chain rounds exactly as fmaf would.
+            float2 acc[VT_FPT / 2][3];
 #pragma unroll
-            for (int q = 0; q < VT_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0f;
-            // sequential fused multiply-add over k for every output (the order the oracle uses)
+            for (int q = 0; q < VT_FPT / 2; ++q) acc[q][0] = acc[q][1] = acc[q][2] = make_float2(0.0f, 0.0f);
             int k = 0;
             for (; k + 4 <= K; k += 4) {
                 const float4 ex = *reinterpret_cast<const float4 *>(er + k);
@@ -326,25 +340,32 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
                 const float exv[4] = {ex.x, ex.y, ex.z, ex.w}, eyv[4] = {ey.x, ey.y, ey.z, ey.w};
                 const float ezv[4] = {ez.x, ez.y, ez.z, ez.w};
 #pragma unroll
-                for (int q = 0; q < VT_FPT; ++q) {
-                    const float4 x4 = *reinterpret_cast<const float4 *>(xr + q * KP + k);
-                    const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
+                for (int jj = 0; jj < 4; ++jj) {
+                    const float4 xa = *reinterpret_cast<const float4 *>(xr + (k + jj) * VT_F);
+                    const float4 xb = *reinterpret_cast<const float4 *>(xr + (k + jj) * VT_F + 4);
+                    const float2 xv[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
+                                          make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
+                    const float2 e0 = make_float2(exv[jj], exv[jj]), e1 = make_float2(eyv[jj], eyv[jj]);
+                    const float2 e2 = make_float2(ezv[jj], ezv[jj]);
 #pragma unroll
-                    for (int jj = 0; jj < 4; ++jj) {
-                        acc[q][0] = fmaf(exv[jj], xv[jj], acc[q][0]);
-                        acc[q][1] = fmaf(eyv[jj], xv[jj], acc[q][1]);
-                        acc[q][2] = fmaf(ezv[jj], xv[jj], acc[q][2]);
+                    for (int q = 0; q < VT_FPT / 2; ++q) {
+                        acc[q][0] = ffma2(e0, xv[q], acc[q][0]);
+                        acc[q][1] = ffma2(e1, xv[q], acc[q][1]);
+                        acc[q][2] = ffma2(e2, xv[q], acc[q][2]);
                     }
                 }
             }
             for (; k < K; ++k) {
                 const float ex = er[k], ey = er[KP + k], ez = er[2 * KP + k];
+                const float4 xa = *reinterpret_cast<const float4 *>(xr + k * VT_F);
+                const float4 xb = *reinterpret_cast<const float4 *>(xr + k * VT_F + 4);
+                const float2 xv[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
+                                      make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
 #pragma unroll
-                for (int q = 0; q < VT_FPT; ++q) {
-                    const float xv = xr[q * KP + k];
-                    acc[q][0] = fmaf(ex, xv, acc[q][0]);
-                    acc[q][1] = fmaf(ey, xv, acc[q][1]);
-                    acc[q][2] = fmaf(ez, xv, acc[q][2]);
+                for (int q = 0; q < VT_FPT / 2; ++q) {
+                    acc[q][0] = ffma2(make_float2(ex, ex), xv[q], acc[q][0]);
+                    acc[q][1] = ffma2(make_float2(ey, ey), xv[q], acc[q][1]);
+                    acc[q][2] = ffma2(make_float2(ez, ez), xv[q], acc[q][2]);
                 }
             }
             __syncwarp();                          // this warp is done with the buffer
@@ -356,7 +377,10 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
                     if (!s_render[fl]) continue;
                     const int f = s_frame[fl];
                     const float *R = Fs + fl * VT_FR, *tau = R + 9, *cam = R + 12;
-                    const float X0 = mx + acc[q][0], Y0 = my + acc[q][1], Z0 = mz + acc[q][2];
+                    const float2 *a = acc[q >> 1];
+                    const float X0 = mx + ((q & 1) ? a[0].y : a[0].x);
+                    const float Y0 = my + ((q & 1) ? a[1].y : a[1].x);
+                    const float Z0 = mz + ((q & 1) ? a[2].y : a[2].x);
                     const float X3 = ((R[0] * X0 + R[3] * Y0) + R[6] * Z0) + tau[0];
                     const float Y3 = ((R[1] * X0 + R[4] * Y0) + R[7] * Z0) + tau[1];
                     const float Z3 = ((R[2] * X0 + R[5] * Y0) + R[8] * Z0) + tau[2];

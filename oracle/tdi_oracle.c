@@ -1235,15 +1235,15 @@ static void orth_rp(const float *R, const float *p0L, int i, float *r)
     for (int k = 0; k < 3; ++k) r[k] = (R[k] * p0 + R[3 + k] * p1) + R[6 + k] * p2;
 }
 
-int o_orthographic_f(const float *xl, const float *yl, const float *p0L, float *x, float *R_last)
+/* The Gauss-Newton iterations of OrthographicInitializer::fit_model from the start point in x
+ * (reset_variables = false continues from x, orthographic_initializer.cu:243-250). */
+static int orth_fit(const float *xl, const float *yl, const float *p0L, float *x, float *R_last)
 {
     float xb[O_NL], yb[O_NL], xm = 0.0f, ym = 0.0f;
     for (int i = 0; i < O_NL; ++i) { xm += xl[i]; ym += yl[i]; }
     xm = xm / (float)O_NL;
     ym = ym / (float)O_NL;
     for (int i = 0; i < O_NL; ++i) { xb[i] = xl[i] - xm; yb[i] = yl[i] - ym; }
-    const float x0[ORTH_N] = {0.0f, 0.0f, 15.0f, 15.0f, 0.0f, 0.0f, 0.05f};
-    for (int n = 0; n < ORTH_N; ++n) x[n] = x0[n];
     for (int k = 0; k < 9; ++k) R_last[k] = 0.0f;
     int terminate = 0, q;
     for (q = 0; q < 100; ++q) {
@@ -1312,4 +1312,12 @@ int o_orthographic_f(const float *xl, const float *yl, const float *p0L, float *
         }
     }
     return q;
+}
+
+int o_orthographic_f(const float *xl, const float *yl, const float *p0L, float *x, float *R_last)
+{
+    /* reset_orthographic (orthographic_initializer.cu:133-153): the reference's start point */
+    const float x0[ORTH_N] = {0.0f, 0.0f, 15.0f, 15.0f, 0.0f, 0.0f, 0.05f};
+    for (int n = 0; n < ORTH_N; ++n) x[n] = x0[n];
+    return orth_fit(xl, yl, p0L, x, R_last);
 }
