@@ -40,6 +40,12 @@ NL = 51                # landmarks per frame (src/lib/constants.h:31)
 DIM = 256              # crop side (src/lib/constants.h:55-56)
 REF_FACE_SIZE = 78.0   # build/configs/BFMmm-19830.cfg1.global4.txt:8
 KERNEL_SIGMA_TAPS = {  # 15-tap tables, src/lib/video_fitter.cu:53-56
+    0.50: [2.15799964e-43, 4.23189662e-32, 1.51709817e-22, 9.96126162e-15, 1.19794565e-08,
+           2.63865077e-04, 1.06450766e-01, 7.86570668e-01, 1.06450766e-01, 2.63865077e-04,
+           1.19794565e-08, 9.96126162e-15, 1.51709817e-22, 4.23189662e-32, 2.15799964e-43],
+    2.00: [4.9640312e-06, 8.9220186e-05, 1.0281866e-03, 7.5973268e-03, 3.5993993e-02,
+           1.0934010e-01, 2.1296541e-01, 2.6596162e-01, 2.1296541e-01, 1.0934010e-01,
+           3.5993993e-02, 7.5973268e-03, 1.0281866e-03, 8.9220186e-05, 4.9640312e-06],
     0.75: [6.4550189e-20, 6.7361578e-15, 1.1880850e-10, 3.5416286e-07, 1.7843490e-04,
            1.5194189e-02, 2.1867350e-01, 5.3190696e-01, 2.1867350e-01, 1.5194189e-02,
            1.7843490e-04, 3.5416286e-07, 1.1880850e-10, 6.7361578e-15, 6.4550189e-20],

@@ -67,6 +67,12 @@ def make_workload(synth, n_frames, seed_offset=0):
     return synth.make_workload(WORKLOAD, n_frames, seed_offset)
 
 
+def shard_range(n_frames, world, rank):
+    """Contiguous frames [f0, f1) of rank `rank` when one video's frames are split over `world`
+    GPUs (frames are independent: no exchange until the outputs are gathered)."""
+    return n_frames * rank // world, n_frames * (rank + 1) // world
+
+
 def max_over_ranks(values, world, device="cpu"):
     """The job's clock: every rank's device times (ms), reduced with MAX over the ranks."""
     import torch
