@@ -66,7 +66,7 @@ class FitConfig(C.Structure):
                 ("twostage_illum", C.c_int32), ("finetune", C.c_int32),
                 ("niters_success", C.c_int32), ("max_iters_lambda", C.c_int32),
                 ("ref_face_size", C.c_float), ("taps", C.c_float * 15), ("normal_eq", C.c_int32),
-                ("damping", C.c_float)]
+                ("damping", C.c_float), ("host_rounds", C.c_int32)]
 
 
 class Report(C.Structure):
@@ -87,6 +87,11 @@ SIGNATURES = {
     "tdi_orthographic_init": (C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tdi_batch_landmark_init": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tdi_batch_loss": (C.c_int32, [C.c_void_p, C.POINTER(FitConfig), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
+    "tdi_batch_loss_backward": (C.c_int32, [C.c_void_p, C.POINTER(FitConfig), C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_fit": (C.c_int32, [C.c_void_p, C.POINTER(FitConfig), C.c_void_p]),
     "tdi_batch_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_fit_frames": (C.c_int32, [C.c_void_p, C.POINTER(FramesDesc), C.POINTER(FitConfig),
@@ -153,16 +158,18 @@ NORMAL_EQ_EXACT, NORMAL_EQ_TENSOR = 0, 1
 
 def default_config(max_iters_rigid=100, max_iters_finetune=100, twostage_illum=0, finetune=0,
                    niters_success=6, max_iters_lambda=10000, ref_face_size=78.0,
-                   kernel_sigma=0.75, normal_eq=NORMAL_EQ_EXACT, damping=0.0) -> FitConfig:
+                   kernel_sigma=0.75, normal_eq=NORMAL_EQ_EXACT, damping=0.0, host_rounds=0) -> FitConfig:
     """Configuration keys of the reference's YAML config (src/lib/config.cu:350-541), plus
     ``normal_eq``: NORMAL_EQ_EXACT (FP64 in the oracle's order) or NORMAL_EQ_TENSOR
     (split-BF16 products on the tensor cores), and ``damping``: the lambda of the damped
-    shape solve (H + lambda I) d = -g; 0 is the reference's undamped solve."""
+    shape solve (H + lambda I) d = -g; 0 is the reference's undamped solve; ``host_rounds``: 1
+    launches every fitting round from the host instead of replaying CUDA graphs of rounds."""
     from . import synth
     c = FitConfig(max_iters_rigid, max_iters_finetune, twostage_illum, finetune, niters_success,
                   max_iters_lambda, ref_face_size)
     c.normal_eq = normal_eq
     c.damping = float(damping)
+    c.host_rounds = int(host_rounds)
     for i, t in enumerate(synth.KERNEL_SIGMA_TAPS[kernel_sigma]):
         c.taps[i] = t
     return c
@@ -267,8 +274,24 @@ class Batch:
         self.n = F
 
     def set_state(self, x, lam, L):
-        x, lam, L = _f32(x), _f32(lam), _f32(L)
-        _check(load_library().tdi_batch_set_state(self.handle, _p(x), _p(lam), _p(L), None))
+        """States x [F][K+6] (None keeps the device states), light lam [F][3] and L [F]."""
+        lam, L = _f32(lam), _f32(L)
+        xp = None
+        if x is not None:
+            x = _f32(x)
+            xp = _p(x)
+        _check(load_library().tdi_batch_set_state(self.handle, xp, _p(lam), _p(L), None))
+
+    def landmark_init(self, p0L):
+        """Landmark initialisation of the batch's frames (tdi_batch_landmark_init) with the
+        orthographic step's landmark points p0L [3][51]. The fitted states stay on the device
+        for the image fit; returns per frame (success, slack, Newton iterations)."""
+        p0L = _f32(p0L)
+        ok = np.zeros(self.n, np.int32)
+        slack = np.zeros(self.n, np.float32)
+        it = np.zeros(self.n, np.int32)
+        _check(load_library().tdi_batch_landmark_init(self.handle, _p(p0L), _p(ok), _p(slack), _p(it), None))
+        return ok.astype(bool), slack, it
 
     def fit(self, cfg: FitConfig, stream=None):
         _check(load_library().tdi_batch_fit(self.handle, C.byref(cfg), stream))

@@ -10,6 +10,8 @@
 #include "tdi_normal_tc.cu"
 #include "tdi_preprocess.cu"
 #include "tdi_orthographic.cu"
+#include "tdi_landmark.cu"
+#include "tdi_adjoint.cu"
 
 #include "../../include/tdi.h"
 
@@ -123,6 +125,7 @@ Cfg to_cfg(const tdi_fit_config &c)
     for (int i = 0; i < NTAPS; ++i) r.taps[i] = c.taps[i];
     r.normal_eq = c.normal_eq;
     r.damping = c.damping;
+    r.host_rounds = c.host_rounds;
     return r;
 }
 
@@ -158,6 +161,10 @@ struct tdi_batch {
     uint8_t *raw_stage = nullptr;  // device copies of raw video frames (tdi_batch_set_video_frames)
     size_t raw_stage_bytes = 0;
     PrepFrame *prep = nullptr;     // [cap] their descriptors
+    float *lm_buf = nullptr;       // landmark initialisation: p0L [3][51], orthographic x [cap][7], R [cap][9], slack [cap]
+    int32_t *lm_ibuf = nullptr;    // its iterations, run flags, successes, Newton steps [4][cap]
+    double *adj = nullptr;         // differentiable loss: FP64 geometry, images, adjoints (tdi_batch_loss)
+    size_t adj_doubles = 0;
     float *ctrl_scratch = nullptr;
     double *scalars = nullptr;     // [cap][4]
     int *d_count = nullptr;
@@ -166,6 +173,14 @@ struct tdi_batch {
     int64_t launches = 0;          // kernels launched by this batch
     int prof_id = 0;               // kernel timed by tdi_batch_profile
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+    // CUDA graphs of GRAPH_ROUNDS rounds of a stage, per (stage, capacity tier, frames, config)
+    struct RoundGraph {
+        int stage, tier, F;
+        Cfg cfg;
+        cudaGraphExec_t exec;
+        int64_t kernels;           // kernel nodes in the graph
+    };
+    std::vector<RoundGraph> graphs;
 };
 
 namespace {
@@ -446,10 +461,88 @@ tdi_status stage_round(tdi_batch *bt, const Cfg &c, int stage, const DBatch &b, 
     return TDI_OK;
 }
 
+// Rounds replayed from CUDA graphs. A graph holds GRAPH_ROUNDS rounds of a stage, each followed by
+// the compaction of the active frames into the device count that the next round's kernels
+// read; grids are sized for a capacity tier (the smallest of 32, 128, 512 or the batch that
+// holds the frames still running: the count only falls during a stage), and blocks past the
+// device count return at once. The host reads the count once per replay instead of once per
+// round. Graphs are built on first use and kept per (stage, tier, frames, configuration).
+constexpr int GRAPH_ROUNDS = 16;
+
+int graph_tier(int n, int F)
+{
+    for (int t : {32, 128, 512})
+        if (n <= t && t < F) return t;
+    return F;
+}
+
+tdi_status stage_graph(tdi_batch *bt, const Cfg &c, int stage, tdi_lane &ln, int tier, tdi_batch::RoundGraph **out)
+{
+    for (auto &g : bt->graphs)
+        if (g.stage == stage && g.tier == tier && g.F == ln.d.F && std::memcmp(&g.cfg, &c, sizeof(Cfg)) == 0) {
+            *out = &g;
+            return TDI_OK;
+        }
+    DBatch gv = ln.d;
+    gv.dnact = ln.d_count;
+    gv.nact = tier;                             // grid sizes only: the kernels read the device count
+    const int64_t before = bt->launches;
+    TDI_CUDA(cudaStreamBeginCapture(ln.s, cudaStreamCaptureModeThreadLocal));
+    tdi_status st = TDI_OK;
+    for (int r = 0; r < GRAPH_ROUNDS && st == TDI_OK; ++r) {
+        st = stage_round(bt, c, stage, gv, ln.s, 1 + r);
+        if (st == TDI_OK)
+            st = launch(bt, 0, k_compact_active, dim3(1), dim3(1024), 0, ln.s, (const DBatch)gv, ln.d_count);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(ln.s, &graph);
+    const int64_t kernels = bt->launches - before;
+    bt->launches = before;
+    if (st != TDI_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+    if (ec != cudaSuccess) return fail(TDI_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(TDI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    bt->graphs.push_back({stage, tier, ln.d.F, c, exec, kernels});
+    *out = &bt->graphs.back();
+    return TDI_OK;
+}
+
+// A stage with its rounds replayed from graphs (one lane, no live profiling).
+tdi_status run_stage_graphs(tdi_batch *bt, const Cfg &c, int stage)
+{
+    const DModel &m = bt->m->d;
+    tdi_lane &ln = bt->lanes[0];
+    TDI_TRY(launch(bt, 0, k_stage_start, dim3((ln.d.F + 127) / 128), dim3(128), 0, ln.s, m, ln.d, c, stage));
+    TDI_TRY(lane_compact(bt, ln));
+    TDI_TRY(lane_count(ln));
+    const long max_rounds = stage == ST_LAMBDA ? 8L * c.max_iters_lambda + 16
+                                               : 16L * (stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune) + 16;
+    long round = 0;
+    if (stage == ST_LAMBDA && ln.n > 0) {       // the light fit's first round also rasterises
+        TDI_TRY(stage_round(bt, c, stage, ln.d, ln.s, 0));
+        TDI_TRY(lane_compact(bt, ln));
+        TDI_TRY(lane_count(ln));
+        round = 1;
+    }
+    while (ln.n > 0 && round < max_rounds) {
+        tdi_batch::RoundGraph *g = nullptr;
+        TDI_TRY(stage_graph(bt, c, stage, ln, graph_tier(ln.n, ln.d.F), &g));
+        TDI_CUDA(cudaGraphLaunch(g->exec, ln.s));
+        bt->launches += g->kernels;
+        TDI_CUDA(cudaMemcpyAsync(ln.h_count, ln.d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, ln.s));
+        TDI_TRY(lane_count(ln));
+        round += GRAPH_ROUNDS;
+    }
+    return TDI_OK;
+}
+
 // A stage (fit_3DMM_lambdas / _shape_rigid / _epsilon_finetune) for every frame of every lane:
 // the lanes' rounds are enqueued on their own streams before any lane is waited for.
 tdi_status run_stage_lanes(tdi_batch *bt, const Cfg &c, int stage, int nlanes)
 {
+    if (nlanes == 1 && !c.host_rounds && bt->prof_id == 0) return run_stage_graphs(bt, c, stage);
     const DModel &m = bt->m->d;
     for (int l = 0; l < nlanes; ++l) {
         tdi_lane &ln = bt->lanes[l];
@@ -685,6 +778,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
 tdi_status tdi_batch_destroy(tdi_batch *b)
 {
     if (!b) return TDI_OK;
+    for (auto &g : b->graphs) cudaGraphExecDestroy(g.exec);
     for (auto &e : b->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     for (auto &ln : b->lanes) {
         if (ln.s) cudaStreamDestroy(ln.s);
@@ -693,6 +787,9 @@ tdi_status tdi_batch_destroy(tdi_batch *b)
     }
     for (void *p : b->allocs) cudaFree(p);
     if (b->raw_stage) cudaFree(b->raw_stage);
+    if (b->lm_buf) cudaFree(b->lm_buf);
+    if (b->lm_ibuf) cudaFree(b->lm_ibuf);
+    if (b->adj) cudaFree(b->adj);
     if (b->h_count) cudaFreeHost(b->h_count);
     delete b;
     return TDI_OK;
@@ -813,17 +910,19 @@ static tdi_status blur_targets(tdi_batch *b, const Cfg &c, cudaStream_t s)
 
 tdi_status tdi_batch_set_state(tdi_batch *b, const float *x, const float *lam, const float *L, void *stream)
 {
-    if (!b || !x || !lam || !L) return fail(TDI_ERR_INVALID, "null state");
+    if (!b || !lam || !L) return fail(TDI_ERR_INVALID, "null state");
     cudaStream_t s = (cudaStream_t)stream;
     const DModel &m = b->m->d;
     const int F = b->d.F;
     std::vector<float> xp((size_t)F * m.KTP, 0.0f), lp((size_t)F * 4, 0.0f);
     for (int f = 0; f < F; ++f) {
-        std::memcpy(&xp[(size_t)f * m.KTP], x + (size_t)f * m.KT, sizeof(float) * m.KT);
+        if (x) std::memcpy(&xp[(size_t)f * m.KTP], x + (size_t)f * m.KT, sizeof(float) * m.KT);
         for (int j = 0; j < 3; ++j) lp[f * 4 + j] = lam[f * 3 + j];
     }
-    TDI_CUDA(cudaMemcpyAsync(b->d.x, xp.data(), sizeof(float) * xp.size(), cudaMemcpyHostToDevice, s));
-    TDI_CUDA(cudaMemcpyAsync(b->d.x_ls, xp.data(), sizeof(float) * xp.size(), cudaMemcpyHostToDevice, s));
+    if (x) {   // NULL keeps the states on the device (after tdi_batch_landmark_init)
+        TDI_CUDA(cudaMemcpyAsync(b->d.x, xp.data(), sizeof(float) * xp.size(), cudaMemcpyHostToDevice, s));
+        TDI_CUDA(cudaMemcpyAsync(b->d.x_ls, xp.data(), sizeof(float) * xp.size(), cudaMemcpyHostToDevice, s));
+    }
     TDI_CUDA(cudaMemcpyAsync(b->d.lam, lp.data(), sizeof(float) * lp.size(), cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync(b->d.lam_ls, lp.data(), sizeof(float) * lp.size(), cudaMemcpyHostToDevice, s));
     TDI_CUDA(cudaMemcpyAsync((void *)b->d.Lint, L, sizeof(float) * F, cudaMemcpyHostToDevice, s));
@@ -969,7 +1068,8 @@ tdi_status tdi_orthographic_init(int32_t n_frames, const float *xl, const float 
         TDI_CUDA(cudaMemcpyAsync(dxl, xl, F * NL * sizeof(float), cudaMemcpyHostToDevice, s));
         TDI_CUDA(cudaMemcpyAsync(dyl, yl, F * NL * sizeof(float), cudaMemcpyHostToDevice, s));
         TDI_CUDA(cudaMemcpyAsync(dp, p0L, 3 * NL * sizeof(float), cudaMemcpyHostToDevice, s));
-        k_orthographic<<<(unsigned)((F + OR_WARPS - 1) / OR_WARPS), OR_WARPS * 32, 0, s>>>(dxl, dyl, dp, n_frames, dx, dR, dit);
+        k_orthographic<<<(unsigned)((F + OR_WARPS - 1) / OR_WARPS), OR_WARPS * 32, 0, s>>>(dxl, dyl, dp, n_frames, dx, dR, dit,
+                                                                                     nullptr, nullptr);
         TDI_CUDA(cudaGetLastError());
         TDI_CUDA(cudaMemcpyAsync(x_out, dx, F * OR_N * sizeof(float), cudaMemcpyDeviceToHost, s));
         TDI_CUDA(cudaMemcpyAsync(R.data(), dR, F * 9 * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -985,6 +1085,166 @@ tdi_status tdi_orthographic_init(int32_t n_frames, const float *xl, const float 
         if (ypr_out) euler_degrees(&R[f * 9], ypr_out + f * 3);
         if (iters_out) iters_out[f] = it[f];
     }
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_landmark_init(tdi_batch *b, const float *p0L, int32_t *success, float *slack, int32_t *iters,
+                                   void *stream)
+{
+    if (!b || !p0L) return fail(TDI_ERR_INVALID, "null argument");
+    const DModel &m = b->m->d;
+    if (m.K + 7 > LM_MAXN) return fail(TDI_ERR_INVALID, "landmark initialisation takes at most 129 expression components");
+    const int F = b->d.F;
+    if (F <= 0) return fail(TDI_ERR_INVALID, "no frames: call tdi_batch_set_frames first");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t cap = (size_t)b->cap;
+    if (!b->lm_buf) {
+        TDI_CUDA(cudaMalloc(&b->lm_buf, sizeof(float) * (3 * NL + cap * (7 + 9 + 1))));
+        if (cudaMalloc(&b->lm_ibuf, sizeof(int32_t) * 4 * cap) != cudaSuccess) {
+            cudaFree(b->lm_buf);
+            b->lm_buf = nullptr;
+            return fail(TDI_ERR_NOMEM, "cudaMalloc");
+        }
+    }
+    float *dp = b->lm_buf, *xo = dp + 3 * NL, *Ro = xo + 7 * cap, *dslack = Ro + 9 * cap;
+    int32_t *dit = b->lm_ibuf, *drun = dit + cap, *dsucc = drun + cap, *dnewton = dsucc + cap;
+    static bool attr = false;
+    if (!attr) {
+        TDI_CUDA(cudaFuncSetAttribute(k_landmark_init, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        attr = true;
+    }
+    const size_t smem = lm_smem(m.K);
+    if (smem > 220 * 1024) return fail(TDI_ERR_INVALID, "too many expression components for the landmark fit");
+    TDI_CUDA(cudaMemcpyAsync(dp, p0L, sizeof(float) * 3 * NL, cudaMemcpyHostToDevice, s));
+    const unsigned ob = (unsigned)((F + OR_WARPS - 1) / OR_WARPS);
+    TDI_TRY(launch(b, 0, k_orthographic, dim3(ob), dim3(OR_WARPS * 32), 0, s, (const float *)b->d.xl,
+                   (const float *)b->d.yl, (const float *)dp, F, xo, Ro, dit, (const float *)nullptr,
+                   (const int32_t *)nullptr));
+    TDI_TRY(launch(b, 0, k_lm_flip, dim3((F + 127) / 128), dim3(128), 0, s, F, xo, (const float *)Ro, drun));
+    TDI_TRY(launch(b, 0, k_orthographic, dim3(ob), dim3(OR_WARPS * 32), 0, s, (const float *)b->d.xl,
+                   (const float *)b->d.yl, (const float *)dp, F, xo, Ro, dit, (const float *)xo, (const int32_t *)drun));
+    TDI_TRY(launch(b, 0, k_landmark_init, dim3(F), dim3(LM_THREADS), smem, s, m, b->d, (const float *)xo, dsucc,
+                   dslack, dnewton));
+    if (success) TDI_CUDA(cudaMemcpyAsync(success, dsucc, sizeof(int32_t) * F, cudaMemcpyDeviceToHost, s));
+    if (slack) TDI_CUDA(cudaMemcpyAsync(slack, dslack, sizeof(float) * F, cudaMemcpyDeviceToHost, s));
+    if (iters) TDI_CUDA(cudaMemcpyAsync(iters, dnewton, sizeof(int32_t) * F, cudaMemcpyDeviceToHost, s));
+    TDI_CUDA(cudaStreamSynchronize(s));
+    if (b->h_count) {
+        int32_t e = 0;
+        TDI_CUDA(cudaMemcpy(&e, b->d.err, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (e) return fail(TDI_ERR_CUDA, "a bounded device-side wait gave up (error word set)");
+    }
+    return TDI_OK;
+}
+
+// Working set of the differentiable loss for cap frames, carved from one FP64 allocation.
+struct AdjBufs {
+    double *geo, *R, *img, *tmp, *B, *T, *adjB, *adjI, *dP0, *dpos, *glob, *geps, *loss;
+};
+
+static tdi_status adj_bufs(tdi_batch *b, AdjBufs &o)
+{
+    const DModel &m = b->m->d;
+    const size_t F = (size_t)b->cap, V = (size_t)m.V;
+    const size_t sizes[13] = {F * V * 8, F * 36, F * NPIX, F * NPIX, F * NPIX, F * NPIX, F * NPIX, F * NPIX,
+                              F * V * 3, F * V * 2, F * AD_GLOB, F * (size_t)m.K, F};
+    size_t total = 0;
+    for (size_t s : sizes) total += (s + 31) / 32 * 32;
+    if (!b->adj) {
+        TDI_CUDA(cudaMalloc(&b->adj, total * sizeof(double)));
+        b->adj_doubles = total;
+    }
+    double **dst[13] = {&o.geo, &o.R, &o.img, &o.tmp, &o.B, &o.T, &o.adjB, &o.adjI, &o.dP0, &o.dpos, &o.glob, &o.geps, &o.loss};
+    double *p = b->adj;
+    for (int i = 0; i < 13; ++i) { *dst[i] = p; p += (sizes[i] + 31) / 32 * 32; }
+    return TDI_OK;
+}
+
+// The raster at the caller's states and the FP64 loss (the forward of the loss and of its adjoint).
+static tdi_status adj_forward(tdi_batch *b, const Cfg &c, const float *x, const float *lam, const float *L,
+                              cudaStream_t s, AdjBufs &o)
+{
+    const DModel &m = b->m->d;
+    DBatch &d = b->d;
+    const int F = d.F;
+    TDI_TRY(adj_bufs(b, o));
+    Launch Lc{b, m, d, s, F};
+    TDI_TRY(launch(b, 0, k_adj_set_x, dim3((F * m.KT + 255) / 256), dim3(256), 0, s, m, d, x, F));
+    TDI_TRY(launch(b, 0, k_fit_begin, Lc.fblocks(), dim3(128), 0, s, d));
+    TDI_TRY(launch(b, 0, k_stage_start, Lc.fblocks(), dim3(128), 0, s, m, d, c, (int)ST_RIGID));
+    int n = 0;
+    TDI_TRY(compact_active(b, s, &n));
+    if (n > 0) {
+        TDI_TRY(launch(b, 0, k_prepare, Lc.wblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
+        TDI_TRY(launch(b, 0, k_compact_render, dim3(1), dim3(1024), 0, s, (const DBatch)d));
+        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, VT_WARPS + 1), Lc.smem_vertex(), s, m, d));
+        TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(raster_blocks(n), n), dim3(RD_THREADS), 0, s, m, d));
+        TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));
+    }
+    const size_t np = (size_t)F * NPIX;
+    const dim3 pb((unsigned)((np + 255) / 256));
+    TDI_TRY(launch(b, 0, k_adj_rot, dim3((F + 127) / 128), dim3(128), 0, s, m, d, x, F, o.R));
+    TDI_TRY(launch(b, 0, k_adj_vertex, dim3((m.V + 255) / 256, F), dim3(256), 0, s, m, x, F, (const double *)o.R,
+                   (const float *)d.cam, o.geo));
+    TDI_CUDA(cudaMemsetAsync(o.img, 0, np * sizeof(double), s));
+    TDI_TRY(launch(b, 0, k_adj_shade, dim3(16, F), dim3(AD_THREADS), 0, s, m, (const DBatch)d, x, lam, L, F,
+                   (const double *)o.geo, (const double *)o.R, o.img));
+    TDI_TRY(launch(b, 0, k_adj_blur, pb, dim3(256), 0, s, (const double *)o.img, o.tmp, c, F, 0));
+    TDI_TRY(launch(b, 0, k_adj_blur, pb, dim3(256), 0, s, (const double *)o.tmp, o.B, c, F, 1));
+    TDI_TRY(launch(b, 0, k_adj_widen, pb, dim3(256), 0, s, (const float *)b->target_raw, o.img, np));
+    TDI_TRY(launch(b, 0, k_adj_blur, pb, dim3(256), 0, s, (const double *)o.img, o.tmp, c, F, 0));
+    TDI_TRY(launch(b, 0, k_adj_blur, pb, dim3(256), 0, s, (const double *)o.tmp, o.T, c, F, 1));
+    TDI_CUDA(cudaMemsetAsync(o.loss, 0, F * sizeof(double), s));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_loss(tdi_batch *b, const tdi_fit_config *cfg, const float *x, const float *lam, const float *L,
+                          double *loss, void *stream)
+{
+    if (!b || !cfg || !x || !lam || !L || !loss) return fail(TDI_ERR_INVALID, "null argument");
+    if (b->d.F <= 0) return fail(TDI_ERR_INVALID, "no frames: call tdi_batch_set_frames first");
+    cudaStream_t s = (cudaStream_t)stream;
+    AdjBufs o;
+    TDI_TRY(adj_forward(b, to_cfg(*cfg), x, lam, L, s, o));
+    const int F = b->d.F;
+    TDI_TRY(launch(b, 0, k_adj_grad, dim3(16, F), dim3(AD_THREADS), 0, s, (const DBatch)b->d, F, (const double *)o.B,
+                   (const double *)o.T, o.loss, (const double *)nullptr, (double *)nullptr));
+    TDI_CUDA(cudaMemcpyAsync(loss, o.loss, F * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return TDI_OK;
+}
+
+tdi_status tdi_batch_loss_backward(tdi_batch *b, const tdi_fit_config *cfg, const float *x, const float *lam,
+                                   const float *L, const double *gloss, double *gx, double *glam, double *gL,
+                                   void *stream)
+{
+    if (!b || !cfg || !x || !lam || !L || !gloss || !gx) return fail(TDI_ERR_INVALID, "null argument");
+    if (b->d.F <= 0) return fail(TDI_ERR_INVALID, "no frames: call tdi_batch_set_frames first");
+    cudaStream_t s = (cudaStream_t)stream;
+    const DModel &m = b->m->d;
+    const Cfg c = to_cfg(*cfg);
+    AdjBufs o;
+    TDI_TRY(adj_forward(b, c, x, lam, L, s, o));   // recomputed: nothing is kept from the forward call
+    const int F = b->d.F;
+    const size_t np = (size_t)F * NPIX;
+    const dim3 pb((unsigned)((np + 255) / 256));
+    TDI_CUDA(cudaMemsetAsync(o.adjB, 0, np * sizeof(double), s));
+    TDI_CUDA(cudaMemsetAsync(o.dP0, 0, (size_t)F * m.V * 3 * sizeof(double), s));
+    TDI_CUDA(cudaMemsetAsync(o.dpos, 0, (size_t)F * m.V * 2 * sizeof(double), s));
+    TDI_CUDA(cudaMemsetAsync(o.glob, 0, (size_t)F * AD_GLOB * sizeof(double), s));
+    TDI_CUDA(cudaMemsetAsync(o.geps, 0, (size_t)F * m.K * sizeof(double), s));
+    TDI_TRY(launch(b, 0, k_adj_grad, dim3(16, F), dim3(AD_THREADS), 0, s, (const DBatch)b->d, F, (const double *)o.B,
+                   (const double *)o.T, o.loss, gloss, o.adjB));
+    // transposed blur: the column pass first, then the row pass
+    TDI_TRY(launch(b, 0, k_adj_blur, pb, dim3(256), 0, s, (const double *)o.adjB, o.tmp, c, F, 1));
+    TDI_TRY(launch(b, 0, k_adj_blur, pb, dim3(256), 0, s, (const double *)o.tmp, o.adjI, c, F, 0));
+    TDI_TRY(launch(b, 0, k_adj_frag_back, dim3(16, F), dim3(AD_THREADS), 0, s, m, (const DBatch)b->d, x, lam, L, F,
+                   (const double *)o.geo, (const double *)o.R, (const double *)o.adjI, o.dP0, o.dpos, o.glob));
+    TDI_TRY(launch(b, 0, k_adj_vertex_back, dim3((m.V + 255) / 256, F), dim3(256), 0, s, m, F, (const double *)o.geo,
+                   (const double *)o.R, (const float *)b->d.cam, (const double *)o.dpos, o.dP0, o.glob));
+    TDI_TRY(launch(b, 0, k_adj_eps, dim3((m.V + AD_VT - 1) / AD_VT, F), dim3(128), 0, s, m, F, (const double *)o.dP0,
+                   o.geps));
+    TDI_TRY(launch(b, 0, k_adj_final, dim3((F + 127) / 128), dim3(128), 0, s, m, F, (const double *)o.R,
+                   (const double *)o.glob, (const double *)o.geps, gx, glam, gL));
     return TDI_OK;
 }
 

@@ -77,6 +77,7 @@ struct Cfg {
     float taps[NTAPS];
     int32_t normal_eq;       // 0: FP64 in the oracle's order; 1: split-BF16 tensor cores
     float damping;           // lambda of the damped shape solve (H + lambda I), 0 = undamped
+    int32_t host_rounds;     // 1: host-driven rounds instead of replayed graphs
 };
 
 // Device view of the model.
@@ -116,7 +117,8 @@ struct DBatch {
     float *R, *dR;           // [F][9], [F][27] of the evaluation point
     FrameCtl *ctl;           // [F]
     int32_t *act;            // [F] frames running the stage at the start of the round, ascending
-    int32_t nact;            // entries of act
+    int32_t nact;            // entries of act (host-driven rounds)
+    const int32_t *dnact;    // when set: entries of act read from device memory (rounds in a CUDA graph)
     int32_t *rlist;          // [F] frames of act that render this round (after the pre-checks)
     int32_t *rcount;         // [F]: rcount[0] = entries of rlist (one counter per view)
     // per-render working set

@@ -84,6 +84,11 @@ __device__ __forceinline__ void prof_count(const DBatch &b, int id, unsigned lon
 // ------------------------------------------------------------------------------------------
 // Stage control.
 
+// Frames running the stage this round: the host's count, or the device count the previous
+// round's compaction wrote (rounds replayed from a CUDA graph, whose grids are sized for a
+// capacity; blocks past the count return at once).
+__device__ __forceinline__ int active_n(const DBatch &b) { return b.dnact ? *b.dnact : b.nact; }
+
 __device__ __forceinline__ bool shape_stage(int stage) { return stage != ST_LAMBDA; }
 
 // Writes x_ls = x + t*d over the first n_upd entries; returns false when tau_z < 0 (the
@@ -155,7 +160,7 @@ __global__ void k_prepare(DModel m, DBatch b, int stage)
 {
     // a warp per frame: the lanes copy the evaluation point, lane 0 forms R(u) and dR/du
     const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (i >= b.nact) return;
+    if (i >= active_n(b)) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     const bool active = ctl.active != 0;
@@ -453,14 +458,14 @@ __global__ void __launch_bounds__(PC_WARPS * 32) k_precheck(DModel m, DBatch b, 
     float *pterm = Es + (size_t)NL * EP + (size_t)PC_WARPS * KP;   // [PC_WARPS][nterm]
     float *lm = pterm + PC_WARPS * nterm + warp * NL * PC_LM;
     // the 51 landmark basis rows, once for the block's frames
-    if (blockIdx.x * PC_WARPS >= b.nact) return;
+    if ((int)(blockIdx.x * PC_WARPS) >= active_n(b)) return;
     for (int q = threadIdx.x; q < NL * 3 * KP; q += PC_WARPS * 32) {
         const int li = q / (3 * KP), o = q - li * 3 * KP;
         Es[li * EP + o] = m.E[(size_t)m.lis[li] * 3 * KP + o];
     }
     __syncthreads();
     const int i = blockIdx.x * PC_WARPS + warp;
-    if (i >= b.nact) return;
+    if (i >= active_n(b)) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active || !ctl.render) return;
@@ -722,6 +727,7 @@ constexpr int RR_WARPS = RR_THREADS / 32;
 
 __global__ void __launch_bounds__(RD_THREADS) k_raster_depth(DModel m, DBatch b)
 {
+    if ((int)blockIdx.y >= active_n(b)) return;
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.render) return;
@@ -786,6 +792,7 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t *s_w, uint32
 
 __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch b)
 {
+    if ((int)blockIdx.x >= active_n(b)) return;
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.render) return;
@@ -1197,6 +1204,7 @@ __device__ __forceinline__ void render_region(const DModel &m, const DBatch &b, 
 
 __global__ void __launch_bounds__(RENDER_THREADS, 2) k_render(DModel m, DBatch b, Cfg c, int stage)
 {
+    if ((int)blockIdx.x >= active_n(b)) return;
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.render) return;
@@ -1222,7 +1230,7 @@ __global__ void __launch_bounds__(RENDER_THREADS, 2) k_render(DModel m, DBatch b
 __global__ void k_decide_shape(DModel m, DBatch b, Cfg c, int stage)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= b.nact) return;
+    if (i >= active_n(b)) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active) return;
@@ -1261,7 +1269,7 @@ __global__ void k_decide_shape(DModel m, DBatch b, Cfg c, int stage)
 __global__ void k_decide_lambda(DModel m, DBatch b, Cfg c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= b.nact) return;
+    if (i >= active_n(b)) return;
     const int f = b.act[i];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.active) return;
@@ -1318,6 +1326,7 @@ __device__ __forceinline__ uint32_t cnt_at(const uint32_t *cnt, int p)
 
 __global__ void __launch_bounds__(1024) k_neighbours(DBatch b, int all_frames)
 {
+    if ((int)blockIdx.x >= active_n(b)) return;
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!(all_frames ? ctl.render : ctl.need_jac)) return;
@@ -1514,6 +1523,7 @@ constexpr int JAC_BPF = 32;                  // blocks per frame
 
 __global__ void __launch_bounds__(JAC_THREADS, 4) k_jacobian(DModel m, DBatch b)
 {
+    if ((int)blockIdx.y >= active_n(b)) return;
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -1749,6 +1759,7 @@ __device__ __forceinline__ void ne_pairs(double (&acc)[NE_TPW][2], const double 
 
 __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
 {
+    if ((int)blockIdx.y >= active_n(b)) return;
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -1842,6 +1853,7 @@ __global__ void __launch_bounds__(NE_THREADS, 2) k_normal_eq(DModel m, DBatch b)
 // Sum of the chunk partials in chunk order: H = tau*S, g = -tau*(column KT of S).
 __global__ void __launch_bounds__(NE_THREADS) k_normal_eq_reduce(DModel m, DBatch b)
 {
+    if ((int)blockIdx.y >= active_n(b)) return;
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -1902,6 +1914,7 @@ __device__ __forceinline__ void bar_hessian(double (&acc)[NE_TPW][2], const floa
 
 __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft_bounds)
 {
+    if ((int)blockIdx.x >= active_n(b)) return;
     const int f = b.act[blockIdx.x];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -2201,6 +2214,7 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
 
 __global__ void __launch_bounds__(SV_THREADS) k_solve(DModel m, DBatch b, Cfg c, int stage)
 {
+    if ((int)blockIdx.x >= active_n(b)) return;
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -2218,6 +2232,7 @@ constexpr int LJ_U = 4;   // fragments per thread whose gathers are in flight to
 
 __global__ void __launch_bounds__(256) k_lambda_jac(DModel m, DBatch b, Cfg c)
 {
+    if ((int)blockIdx.x >= active_n(b)) return;
     const int f = b.act[blockIdx.x];
     FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -2380,9 +2395,10 @@ __global__ void __launch_bounds__(1024) k_compact_render(DBatch b)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_base = 0;
     __syncthreads();
-    for (int i0 = 0; i0 < b.nact; i0 += 1024) {
+    const int na = active_n(b);
+    for (int i0 = 0; i0 < na; i0 += 1024) {
         const int i = i0 + tid;
-        const int f = i < b.nact ? b.act[i] : -1;
+        const int f = i < na ? b.act[i] : -1;
         const int r = f >= 0 && b.ctl[f].render;
         const unsigned mask = __ballot_sync(0xffffffffu, r);
         if (lane == 0) s_warp[warp] = __popc(mask);

@@ -107,6 +107,7 @@ __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b)
 template <int GRP>
 __global__ void __launch_bounds__(TC_THREADS, 3) k_normal_eq_tc(DModel m, DBatch b)
 {
+    if ((int)blockIdx.y >= active_n(b)) return;
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;
@@ -259,6 +260,7 @@ constexpr int TC_RBLOCKS = 4;
 
 __global__ void __launch_bounds__(256) k_normal_eq_tc_reduce(DModel m, DBatch b)
 {
+    if ((int)blockIdx.y >= active_n(b)) return;
     const int f = b.act[blockIdx.y];
     const FrameCtl &ctl = b.ctl[f];
     if (!ctl.need_jac) return;

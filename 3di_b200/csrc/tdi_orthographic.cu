@@ -70,13 +70,17 @@ __device__ void orth_solve(const float *H, const float *g, float *d)
     for (int i = 0; i < OR_N; ++i) d[i] = (float)(-y[i]);
 }
 
+// x_start: NULL for the reference's start point (reset_orthographic), else [F][7] start points
+// (fit_model with reset_variables = false); run: NULL, or [F] flags selecting the frames fitted.
 __global__ void __launch_bounds__(OR_WARPS * 32) k_orthographic(const float *xl, const float *yl, const float *p0L,
-                                                                int F, float *x_out, float *R_out, int32_t *iters)
+                                                                int F, float *x_out, float *R_out, int32_t *iters,
+                                                                const float *x_start, const int32_t *run)
 {
     __shared__ OrthWarp sw[OR_WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = blockIdx.x * OR_WARPS + warp;
     if (f >= F) return;
+    if (run && !run[f]) return;
     OrthWarp &w = sw[warp];
     const float *xf = xl + (size_t)f * NL, *yf = yl + (size_t)f * NL;
     float xm = 0.0f, ym = 0.0f;
@@ -85,7 +89,7 @@ __global__ void __launch_bounds__(OR_WARPS * 32) k_orthographic(const float *xl,
         xm = xm / (float)NL;
         ym = ym / (float)NL;
         const float x0[OR_N] = {0.0f, 0.0f, 15.0f, 15.0f, 0.0f, 0.0f, 0.05f};
-        for (int n = 0; n < OR_N; ++n) w.x[n] = x0[n];
+        for (int n = 0; n < OR_N; ++n) w.x[n] = x_start ? x_start[(size_t)f * OR_N + n] : x0[n];
         for (int k = 0; k < 9; ++k) w.Rt[k] = 0.0f;
     }
     xm = __shfl_sync(0xffffffffu, xm, 0);

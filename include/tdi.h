@@ -124,6 +124,10 @@ typedef struct {
                                   * system (H + lambda I) d = -g, lambda >= 0 added in FP64 to the
                                   * diagonal before the factorisation. 0 = the reference's undamped
                                   * solve (Solver::solve, solver.h:70-105). */
+    int32_t host_rounds;         /* 0: the fitting rounds of a stage are replayed on the device from
+                                  * CUDA graphs of 16 rounds, the host reading the active-frame count
+                                  * once per replay; 1: the host launches every round and reads the
+                                  * count after each (the same kernels and results). */
 } tdi_fit_config;
 
 typedef struct {
@@ -158,9 +162,26 @@ tdi_status tdi_batch_set_frames(tdi_batch *b, const tdi_frames *frames, void *st
  * Synchronous. */
 tdi_status tdi_batch_set_video_frames(tdi_batch *b, const tdi_video_frames *frames, void *stream);
 /* Upload states: x [F][K+6] (epsilon, tau_x, tau_y, tau_z, u1, u2, u3), lam [F][3],
- * light intensity L [F]. Synchronous. */
+ * light intensity L [F]. x may be NULL: the states on the device stay (after
+ * tdi_batch_landmark_init); only the light is set. Synchronous. */
 tdi_status tdi_batch_set_state(tdi_batch *b, const float *x, const float *lam, const float *L,
                                void *stream);
+/* Landmark initialisation of the batch's frames (after tdi_batch_set_frames or
+ * tdi_batch_set_video_frames), what VideoFitter::fit_to_video_frame runs before the image fit
+ * (video_fitter.cu:456-500): per frame the orthographic pose fit to the landmarks with the
+ * landmark points p0L [3][51] (p0L_mat.dat; tdi_orthographic_init's method, refitted from the
+ * Euler angles when it ends mirrored), its perspective start, the smallest feasible slack and
+ * the log-barrier fit of pose and expressions to the landmark boxes with a slack variable
+ * (Logbarrier_Initializer::initialize_with_orthographic_t, set_minimal_slack, fit_model;
+ * logbarrier_initializer.cu:1041-1269,1862-1918). The expression bounds are the model's shape-fit
+ * bounds; the landmark 3D points are the model's mean and expression basis at its landmarks.
+ * Writes the batch's states on the device (the start of tdi_batch_fit; set the light with
+ * tdi_batch_set_state(b, NULL, lam, L)); per frame (host arrays, each may be NULL): success [F]
+ * (1 when the slack went below -0.01, the reference's fit_success), the final slack [F] and the
+ * Newton iterations [F]. Synchronous. */
+tdi_status tdi_batch_landmark_init(tdi_batch *b, const float *p0L, int32_t *success, float *slack,
+                                   int32_t *iters, void *stream);
+
 /* Fit every frame of the batch on the device (asynchronous on the stream apart from one
  * 4-byte read-back per round). Replaces fit_to_video_frame's fitting calls. */
 tdi_status tdi_batch_fit(tdi_batch *b, const tdi_fit_config *cfg, void *stream);
@@ -204,6 +225,26 @@ tdi_status tdi_batch_raster(tdi_batch *b, int32_t frame, const float *xp, const 
  * the blur (renderer.cu:635-696): unblurred image [F][65536] and the triangle that owns each
  * pixel [F][65536] (-1 where nothing is drawn). Either output may be NULL. Synchronous. */
 tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void *stream);
+
+/* Differentiable render loss of every frame of the batch (after tdi_batch_set_frames), for the
+ * torch.autograd.Function of the Python package; no counterpart in the reference, whose fit uses
+ * the warp-only Jacobian contracted with the residual (derivative_computer.cu:157-164).
+ * loss[f] = -sum_n (gxn_n gxsn_n + gyn_n gysn_n): the negated correlation of the normalised
+ * gradients of the blurred render and target at the frame's fragments (funcs.cu:842-897), the
+ * image term the shape fit minimises (scaled there by tau_img = 25). The fragments (triangle and
+ * pixel of every sample, the owner of every pixel) come from the library's raster at x and are
+ * then held; barycentrics, geometry, shading, blur and gradients are FP64 functions of
+ * (epsilon, tau, u, lambda, L), so the loss is smooth in them. DEVICE pointers: x [F][K+6],
+ * lam [F][3], L [F] (float), loss [F] (double); cfg supplies the blur taps. Asynchronous on the
+ * stream except one 8-byte read-back. */
+tdi_status tdi_batch_loss(tdi_batch *b, const tdi_fit_config *cfg, const float *x, const float *lam,
+                          const float *L, double *loss, void *stream);
+/* Gradient of sum_f gloss[f] loss[f] by the hand-written adjoint (raster and FP64 forward
+ * recomputed, nothing stored between the calls): gx [F][K+6] (epsilon, tau, u), glam [F][3] and
+ * gL [F] (double, DEVICE pointers; glam, gL may be NULL). */
+tdi_status tdi_batch_loss_backward(tdi_batch *b, const tdi_fit_config *cfg, const float *x, const float *lam,
+                                   const float *L, const double *gloss, double *gx, double *glam, double *gL,
+                                   void *stream);
 
 /* Kernels launched by this batch since it was created (each a hand-written CUDA kernel). */
 tdi_status tdi_batch_launches(tdi_batch *b, int64_t *launches);

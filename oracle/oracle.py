@@ -65,6 +65,7 @@ def lib(kind: str = "f32") -> C.CDLL:
         L.o_render_image_f.restype = C.c_int
         L.o_vertex_stage_f.restype = C.c_int
         L.o_image_terms_f.restype = C.c_int
+        L.o_landmark_init_f.restype = C.c_int
         L.o_max_threads.restype = C.c_int
         _LIBS[kind] = L
     return _LIBS[kind]
@@ -252,6 +253,18 @@ def render_target(model: Model, fr, i: int, cfg: OConfig, x, lam, L, kind="f32")
     N = lib(kind).o_render_image_f(C.byref(model.s), C.byref(f), C.byref(cfg), _p(_f32(x)),
                                    _p(_f32(lam)), C.c_float(float(L)), _p(tgt), C.byref(flags))
     return tgt, N, flags.value
+
+
+def landmark_init(model: Model, frames: FrameSet, j: int, p0L, kind="f32"):
+    """Landmark initialisation of frame j (orthographic step, perspective start, barrier method
+    with a slack variable). Returns (x [K+6], slack, success, newton iterations, mirrored)."""
+    x = np.zeros(model.K + 6, np.float32)
+    slack = C.c_float(0)
+    newton = C.c_int(0)
+    flip = C.c_int(0)
+    ok = lib(kind).o_landmark_init_f(C.byref(model.s), C.byref(frames.arr[j]), _p(_f32(p0L)), _p(x),
+                                     C.byref(slack), C.byref(newton), C.byref(flip))
+    return x, slack.value, bool(ok), newton.value, bool(flip.value)
 
 
 def max_threads(kind="f32") -> int:

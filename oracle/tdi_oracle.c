@@ -1321,3 +1321,322 @@ int o_orthographic_f(const float *xl, const float *yl, const float *p0L, float *
     for (int n = 0; n < ORTH_N; ++n) x[n] = x0[n];
     return orth_fit(xl, yl, p0L, x, R_last);
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* Landmark initialisation of one frame, as VideoFitter::fit_to_video_frame runs it before the
+ * image fit (video_fitter.cu:456-500): Logbarrier_Initializer::initialize_with_orthographic_t
+ * (logbarrier_initializer.cu:1862-1918), set_minimal_slack (:1041-1092) and fit_model with a
+ * slack variable (:1095-1269; compute_gradient_and_hessian :1272-1843, evaluate_objective_function
+ * :1921-2093, compute_Gs :456-520, fill_optimization_dc_landmark :587-697,
+ * fill_optimization_dI_depsilon_landmark :836-912, fill_for_nabla2F_dsdc :780-818). One frame,
+ * no identity, no smoothing or expression regularisation (the video fit's initializer,
+ * video_fitter.cu:30). Unknowns z = (epsilon[K], tau[3], u[3], s): the barrier method minimises
+ * tau_lb s - sum log(G) - sum log(bound gaps) with G = s - (constraint gap) and stops once
+ * s < -0.01 (every landmark inside its box by a margin). Sums over landmarks and constraint rows
+ * (cuBLAS in the reference) are FP64 in a fixed order: rows in the order G_x-, G_y-, G_x+, G_y+,
+ * landmarks ascending within each; the Hessian is an FMA chain over those rows. */
+
+#define LM_ROWS (4 * O_NL)
+#define LM_PI 3.14159265358979323846   /* M_PI of <math.h> (not declared under -std=c11) */
+
+typedef struct {
+    real G[LM_ROWS];          /* G_x-, G_y-, G_x+, G_y+ */
+    real invG[LM_ROWS];       /* 1 / (1e-6 + G) */
+    real nlog[LM_ROWS];       /* -log G */
+    real *F;                  /* [LM_ROWS][n]: constraint rows of the barrier derivative */
+    real *nWx, *nWy;          /* [O_NL][n - 1]: projection derivatives */
+    real R[9], dR[27];
+} lm_terms_t;
+
+/* compute_nonrigid_shape + compute_Gs + the derivative kernels at z. */
+static void lm_terms(const o_model *m, const o_frame *f, const real *z, int deriv, lm_terms_t *o)
+{
+    const int K = m->K, V = m->V, n = K + 7;
+    const real *tau = z + K, s = z[K + 6];
+    const real phix = f->phix, phiy = f->phiy, cx = f->cx, cy = f->cy, fs = f->face_size;
+    o_rotation(z + K + 3, o->R, deriv ? o->dR : NULL);
+    const real *R = o->R;
+    real p[O_NL * 3], Rp[O_NL * 3];
+    for (int i = 0; i < O_NL; ++i) {
+        const int v = m->lis[i];
+        for (int c = 0; c < 3; ++c) {
+            const float *e = m->E + ((size_t)v * 3 + c) * K;
+            real acc = 0;
+            for (int k = 0; k < K; ++k) acc = RFMA((real)e[k], z[k], acc);
+            p[i * 3 + c] = (real)m->mean[c * V + v] + acc;
+        }
+        for (int r = 0; r < 3; ++r)
+            Rp[i * 3 + r] = (R[r] * p[i * 3] + R[r + 3] * p[i * 3 + 1]) + R[r + 6] * p[i * 3 + 2];
+    }
+    for (int i = 0; i < O_NL; ++i) {
+        const real r1p = Rp[i * 3], r2p = Rp[i * 3 + 1], r3p = Rp[i * 3 + 2];
+        const real xproj = phix * ((r1p + tau[0]) / (r3p + tau[2])) + cx;
+        const real yproj = phiy * ((r2p + tau[1]) / (r3p + tau[2])) + cy;
+        const real xl = f->xl[i], yl = f->yl[i];
+        o->G[0 * O_NL + i] = s - ((xl + (real)f->bounds[0 * O_NL + i] * fs) - xproj);
+        o->G[1 * O_NL + i] = s - ((yl + (real)f->bounds[1 * O_NL + i] * fs) - yproj);
+        o->G[2 * O_NL + i] = s - ((xproj - (real)f->bounds[2 * O_NL + i] * fs) - xl);
+        o->G[3 * O_NL + i] = s - ((yproj - (real)f->bounds[3 * O_NL + i] * fs) - yl);
+    }
+    for (int r = 0; r < LM_ROWS; ++r) {
+        o->invG[r] = (real)1 / ((real)0.000001f + o->G[r]);
+        o->nlog[r] = -RLOG(o->G[r]);
+    }
+    if (!deriv) return;
+    for (int i = 0; i < O_NL; ++i) {
+        const real px = p[i * 3], py = p[i * 3 + 1], pz = p[i * 3 + 2];
+        const real vx = Rp[i * 3] + tau[0], vy = Rp[i * 3 + 1] + tau[1], vz = Rp[i * 3 + 2] + tau[2];
+        const real ivz = (real)1 / vz, ivz2 = ivz * ivz;
+        real *wx = o->nWx + (size_t)i * (n - 1), *wy = o->nWy + (size_t)i * (n - 1);
+        const float *ex = m->E + (size_t)m->lis[i] * 3 * K;
+        for (int k = 0; k < K; ++k) {
+            real RIX = ex[k], RIY = ex[K + k], RIZ = ex[2 * K + k];
+            real dvx = (RIX * R[0] + RIY * R[3]) + RIZ * R[6];
+            real dvy = (RIX * R[1] + RIY * R[4]) + RIZ * R[7];
+            real dvz = (RIX * R[2] + RIY * R[5]) + RIZ * R[8];
+            wx[k] = (phix * ivz2) * (dvx * vz - dvz * vx);
+            wy[k] = (phiy * ivz2) * (dvy * vz - dvz * vy);
+        }
+        wx[K + 0] = phix * ivz; wx[K + 1] = 0; wx[K + 2] = ((-phix) * vx) * ivz2;
+        wy[K + 0] = 0; wy[K + 1] = phiy * ivz; wy[K + 2] = ((-phiy) * vy) * ivz2;
+        for (int a = 0; a < 3; ++a) {
+            const real *d = o->dR + 9 * a;
+            real dvx = (d[0] * px + d[3] * py) + d[6] * pz;
+            real dvy = (d[1] * px + d[4] * py) + d[7] * pz;
+            real dvz = (d[2] * px + d[5] * py) + d[8] * pz;
+            wx[K + 3 + a] = (phix * ivz2) * (vz * dvx - vx * dvz);
+            wy[K + 3 + a] = (phiy * ivz2) * (vz * dvy - vy * dvz);
+        }
+        for (int a = 0; a < n - 1; ++a) {
+            o->F[(size_t)(0 * O_NL + i) * n + a] = (-wx[a]) / o->G[0 * O_NL + i];
+            o->F[(size_t)(1 * O_NL + i) * n + a] = (-wy[a]) / o->G[1 * O_NL + i];
+            o->F[(size_t)(2 * O_NL + i) * n + a] = wx[a] / o->G[2 * O_NL + i];
+            o->F[(size_t)(3 * O_NL + i) * n + a] = wy[a] / o->G[3 * O_NL + i];
+        }
+        for (int q = 0; q < 4; ++q) o->F[(size_t)(q * O_NL + i) * n + n - 1] = 0;
+    }
+}
+
+/* tau_lb s + expression-bound and constraint barrier terms (evaluate_objective_function),
+ * FP64 sums in the order of the reference's accumulations, rounded to REAL. */
+static real lm_objective(const o_model *m, const real *z, real tau, const lm_terms_t *o)
+{
+    const int K = m->K;
+    double acc = (double)(tau * z[K + 6]);
+    double sl = 0.0, su = 0.0, sg = 0.0;
+    for (int k = 0; k < K; ++k) sl += (double)(-RLOG(-((real)m->eps_lb[k] - z[k])));
+    for (int k = 0; k < K; ++k) su += (double)(-RLOG(-(z[k] - (real)m->eps_ub[k])));
+    for (int r = 0; r < LM_ROWS; ++r) sg += (double)o->nlog[r];
+    acc += sl;
+    acc += su;
+    acc += sg;
+    return (real)acc;
+}
+
+/* Gradient g [n] and Hessian H [n][n] (row-major, symmetric) of the barrier problem at the
+ * terms o (compute_gradient_and_hessian with use_slack). */
+static void lm_grad_hess(const o_model *m, const real *z, real tau, const lm_terms_t *o, real *g, real *H)
+{
+    const int K = m->K, n = K + 7, nb = n - 1;
+    for (int a = 0; a < nb; ++a) {
+        /* nablaF: the four rows of each landmark added elementwise (cublasSgeam), then summed
+         * over the landmarks */
+        double acc = 0.0;
+        for (int i = 0; i < O_NL; ++i) {
+            real e = o->F[(size_t)(0 * O_NL + i) * n + a];
+            e = e + o->F[(size_t)(1 * O_NL + i) * n + a];
+            e = e + o->F[(size_t)(2 * O_NL + i) * n + a];
+            e = e + o->F[(size_t)(3 * O_NL + i) * n + a];
+            acc += (double)e;
+        }
+        g[a] = (real)acc;
+    }
+    for (int k = 0; k < K; ++k) {              /* update_gradient (:915-929) */
+        const real fub = z[k] - (real)m->eps_ub[k], flb = (real)m->eps_lb[k] - z[k];
+        g[k] = g[k] + ((real)-1 / fub + (real)1 / flb);
+    }
+    {
+        double acc = 0.0;
+        for (int r = 0; r < LM_ROWS; ++r) acc += (double)o->invG[r];
+        g[nb] = (real)(-acc);
+        g[nb] = tau + g[nb];
+    }
+    for (int a = 0; a < nb; ++a)
+        for (int b = 0; b <= a; ++b) {
+            double acc = 0.0;
+            for (int r = 0; r < LM_ROWS; ++r)
+                acc = fma((double)o->F[(size_t)r * n + a], (double)o->F[(size_t)r * n + b], acc);
+            H[(size_t)a * n + b] = H[(size_t)b * n + a] = (real)acc;
+        }
+    for (int k = 0; k < K; ++k) {              /* update_diagonal_of_hessian_wbounds (:932-949) */
+        const real fub = z[k] - (real)m->eps_ub[k], flb = (real)m->eps_lb[k] - z[k];
+        const real nu = (real)(-1.0 / ((double)fub + 1e-12));
+        const real nl = (real)(1.0 / ((double)flb + 1e-12));
+        H[(size_t)k * n + k] = H[(size_t)k * n + k] + (nu * nu + nl * nl);
+    }
+    for (int a = 0; a < nb; ++a) {             /* fill_for_nabla2F_dsdc + bottom and right */
+        double acc = 0.0;
+        for (int i = 0; i < O_NL; ++i) {
+            const real gxm = o->G[i], gym = o->G[O_NL + i], gxp = o->G[2 * O_NL + i], gyp = o->G[3 * O_NL + i];
+            const real wx = o->nWx[(size_t)i * nb + a], wy = o->nWy[(size_t)i * nb + a];
+            real e = (-wx) / (gxp * gxp) - wy / (gyp * gyp);
+            e = e + wx / (gxm * gxm);
+            e = e + wy / (gym * gym);
+            acc += (double)e;
+        }
+        H[(size_t)nb * n + a] = H[(size_t)a * n + nb] = (real)acc;
+    }
+    {
+        double acc = 0.0;
+        for (int r = 0; r < LM_ROWS; ++r) acc = fma((double)o->invG[r], (double)o->invG[r], acc);
+        H[(size_t)nb * n + nb] = (real)acc;
+    }
+}
+
+/* Euler angles in degrees of the rotation (RotationComputer::compute_euler_angles,
+ * rotation_header.cu:421-449, with RAD2DEG of constants.h:59): atan2 in double, rounded. */
+static void lm_euler_deg(const float *R, float *yaw, float *pitch, float *roll)
+{
+    const float c = sqrtf(R[5] * R[5] + R[8] * R[8]);
+    float y, p, r;
+    if (!(c < 1e-6f)) {
+        r = (float)atan2((double)R[1], (double)R[0]);
+        y = (float)atan2((double)-R[2], (double)c);
+        p = (float)atan2((double)R[5], (double)R[8]);
+    } else {
+        r = (float)atan2((double)-R[7], (double)R[4]);
+        y = (float)atan2((double)-R[2], (double)c);
+        p = 0.0f;
+    }
+    *yaw = (float)((double)(y * 180.0f) / LM_PI);
+    *pitch = (float)((double)(p * 180.0f) / LM_PI);
+    *roll = (float)((double)(r * 180.0f) / LM_PI);
+}
+
+/* The start rotation of the second orthographic fit when the first one converged to a mirrored
+ * solution (sigma_x < 0, logbarrier_initializer.cu:1872-1896): the Euler angles (roll, -pitch,
+ * -yaw) as a rotation R = Rz Ry Rx (eulerAnglesToRotationMatrix, newfuncs.cu:720-747) turned
+ * into an axis-angle vector (cv::Rodrigues). OpenCV's float matrix product and its Rodrigues
+ * (an SVD re-orthonormalisation, then the axis from the skew part) are evaluated here in
+ * double from the same float angles: theta = acos((trace - 1) / 2), axis = (R32 - R23,
+ * R13 - R31, R21 - R12) / (2 sin theta), and for theta near pi the axis from the diagonal. */
+static void lm_flip_rotation(float yaw, float pitch, float roll, float *u)
+{
+    const float th[3] = {(float)(((double)roll * LM_PI) / 180.0), (float)(((double)(-pitch) * LM_PI) / 180.0),
+                         (float)(((double)(-yaw) * LM_PI) / 180.0)};
+    /* cos and sin of the float angles in double, rounded to float (the float overloads the
+     * reference calls) */
+    const double c0 = (float)cos((double)th[0]), s0 = (float)sin((double)th[0]);
+    const double c1 = (float)cos((double)th[1]), s1 = (float)sin((double)th[1]);
+    const double c2 = (float)cos((double)th[2]), s2 = (float)sin((double)th[2]);
+    const double Rx[9] = {1, 0, 0, 0, c0, -s0, 0, s0, c0};       /* row-major */
+    const double Ry[9] = {c1, 0, s1, 0, 1, 0, -s1, 0, c1};
+    const double Rz[9] = {c2, -s2, 0, s2, c2, 0, 0, 0, 1};
+    double T[9], R[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T[i * 3 + j] = 0;
+            for (int k = 0; k < 3; ++k) T[i * 3 + j] += Ry[i * 3 + k] * Rx[k * 3 + j];
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            R[i * 3 + j] = 0;
+            for (int k = 0; k < 3; ++k) R[i * 3 + j] += Rz[i * 3 + k] * T[k * 3 + j];
+        }
+    const double rx = R[7] - R[5], ry = R[2] - R[6], rz = R[3] - R[1];
+    const double sn = 0.5 * sqrt(rx * rx + ry * ry + rz * rz);
+    double cs = 0.5 * (R[0] + R[4] + R[8] - 1.0);
+    cs = cs > 1.0 ? 1.0 : (cs < -1.0 ? -1.0 : cs);
+    const double theta = acos(cs);
+    double out[3];
+    if (sn < 1e-5) {
+        if (cs > 0) { out[0] = out[1] = out[2] = 0.0; }
+        else {
+            double ax = sqrt((R[0] + 1) * 0.5), ay = sqrt((R[4] + 1) * 0.5), az = sqrt((R[8] + 1) * 0.5);
+            if (R[1] < 0) ay = -ay;
+            if (R[2] < 0) az = -az;
+            if (fabs(ax) < fabs(ay) && fabs(ax) < fabs(az) && (R[5] > 0) != (ay * az > 0)) az = -az;
+            out[0] = ax * theta; out[1] = ay * theta; out[2] = az * theta;
+        }
+    } else {
+        const double v = theta / (2.0 * sn);
+        out[0] = rx * v; out[1] = ry * v; out[2] = rz * v;
+    }
+    for (int k = 0; k < 3; ++k) u[k] = (float)out[k];
+}
+
+/* Landmark initialisation of one frame. p0L [3][51]: the orthographic step's landmark points
+ * (p0L_mat.dat). Writes z_out [K+6] (epsilon, tau, u) and the final slack; returns 1 when
+ * the barrier method reached s < -0.01 (fit_success), 0 otherwise. *newton counts the
+ * Newton iterations, *orth_flip whether the mirrored-solution branch ran. */
+int o_landmark_init_f(const o_model *m, const o_frame *f, const float *p0L, float *z_out, float *slack_out,
+                      int *newton, int *orth_flip)
+{
+    const int K = m->K, n = K + 7;
+    /* initialize_with_orthographic_t (:1862-1918) */
+    float xo[ORTH_N], Rl[9], yaw, pitch, roll;
+    o_orthographic_f(f->xl, f->yl, p0L, xo, Rl);
+    lm_euler_deg(Rl, &yaw, &pitch, &roll);
+    *orth_flip = 0;
+    if (xo[2] < 0) {
+        float u0[3];
+        lm_flip_rotation(yaw, pitch, roll, u0);
+        xo[0] = -xo[0];
+        xo[2] = -xo[2];
+        xo[4] = u0[0]; xo[5] = u0[1]; xo[6] = u0[2];
+        orth_fit(f->xl, f->yl, p0L, xo, Rl);
+        *orth_flip = 1;
+    }
+    float xm = 0.0f, ym = 0.0f;                 /* thrust::reduce on the host, then / 51 */
+    for (int i = 0; i < O_NL; ++i) { xm += f->xl[i]; ym += f->yl[i]; }
+    xm = xm / (float)O_NL;
+    ym = ym / (float)O_NL;
+    /* initialize_kernel (:31-51) */
+    const float tz = (float)((double)f->phix / ((double)(fabsf(xo[2]) + fabsf(xo[3])) * 0.5));
+    real *z = (real *)calloc((size_t)n, sizeof(real)), *zt = (real *)calloc((size_t)n, sizeof(real));
+    z[K + 2] = tz;
+    z[K + 0] = (float)((tz * (xm - f->cx)) / f->phix);
+    z[K + 1] = (float)((tz * (ym - f->cy)) / f->phiy);
+    z[K + 3] = xo[4]; z[K + 4] = xo[5]; z[K + 5] = xo[6];
+    lm_terms_t o;
+    o.F = (real *)malloc(sizeof(real) * LM_ROWS * (size_t)n);
+    o.nWx = (real *)malloc(sizeof(real) * O_NL * (size_t)n);
+    o.nWy = (real *)malloc(sizeof(real) * O_NL * (size_t)n);
+    real *H = (real *)malloc(sizeof(real) * (size_t)n * n), *g = (real *)malloc(sizeof(real) * n);
+    real *d = (real *)malloc(sizeof(real) * n);
+    /* set_minimal_slack (:1041-1092): with s = 0, s0 = 5 - min G */
+    z[K + 6] = 0;
+    lm_terms(m, f, z, 0, &o);
+    real gmin = o.G[0];
+    for (int r = 1; r < LM_ROWS; ++r) gmin = o.G[r] < gmin ? o.G[r] : gmin;
+    z[K + 6] = (real)5.0f - gmin;
+    /* fit_model (:1095-1269) */
+    real tau = (real)10.0f;
+    int success = 0, iters = 0;
+    for (int stage = 0; stage < 5 && !success; ++stage) {
+        tau = tau * (real)10.0f;
+        int terminate = 0;
+        for (int it = 0; it < 100 && !terminate; ++it) {
+            if (z[K + 6] < (real)-0.01f) { success = 1; break; }
+            lm_terms(m, f, z, 1, &o);
+            const real obj = lm_objective(m, z, tau, &o);
+            lm_grad_hess(m, z, tau, &o, g, H);
+            ++iters;
+            if (!solve(H, g, n, d, 0.0f)) { terminate = 1; break; }
+            real t = (real)1.0f;
+            for (int inner = 0; inner < 100; ++inner) {
+                if (t < (real)0.01f) { terminate = 1; break; }
+                for (int a = 0; a < n; ++a) zt[a] = z[a] + t * d[a];
+                lm_terms(m, f, zt, 0, &o);
+                const real ot = lm_objective(m, zt, tau, &o);
+                if (ot < obj) { memcpy(z, zt, sizeof(real) * n); break; }
+                t = t * (real)0.5f;
+            }
+        }
+    }
+    for (int a = 0; a < K + 6; ++a) z_out[a] = (float)z[a];
+    *slack_out = (float)z[K + 6];
+    *newton = iters;
+    free(o.F); free(o.nWx); free(o.nWy); free(H); free(g); free(d); free(z); free(zt);
+    return success;
+}

@@ -185,3 +185,24 @@ def test_tensor_core_fit_reaches_the_exact_fits_objective(tdi, synth, O, small_c
         pose_err.append(float((np.abs(x1[i, K:] - x0[i, K:]) / np.maximum(np.abs(x0[i, K:]), 1e-2)).max()))
     print("tensor vs exact fit, pose relative difference per frame:", pose_err)
     assert np.median(pose_err) <= 2e-2 and max(pose_err) <= 1e-1
+
+
+@pytest.mark.parametrize("case_name", ["small_case", "full_case"])
+def test_graph_rounds_equal_host_rounds(request, tdi, synth, O, case_name):
+    """Stage rounds replayed from CUDA graphs (the default: kernels read the active-frame count
+    from device memory, the host reads it once per 16 rounds) give the fits of host-driven
+    rounds bit for bit, including the two-stage illumination and the finetune."""
+    case = request.getfixturevalue(case_name)
+    m, fr, om = case
+    model, batch, lam, L = _setup(tdi, case, synth)
+    kw = dict(max_iters_rigid=10, max_iters_finetune=10, twostage_illum=1, finetune=1)
+    n0 = batch.launches()
+    xg, lg, rg = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(**kw))
+    n1 = batch.launches()
+    xh, lh, rh = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(host_rounds=1, **kw))
+    assert np.array_equal(xg.view(np.uint32), xh.view(np.uint32))
+    assert np.array_equal(lg.view(np.uint32), lh.view(np.uint32))
+    for a, b in zip(rg, rh):
+        assert (a.flags, a.iters_rigid, a.iters_finetune, a.iters_lambda, a.renders) == \
+               (b.flags, b.iters_rigid, b.iters_finetune, b.iters_lambda, b.renders)
+    assert n1 > n0
