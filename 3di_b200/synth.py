@@ -3,6 +3,11 @@
 The BFM'09 files that 3DI fits with are licence-gated and absent, so every input here
 is generated from a seed with the shapes and value distributions of the real model:
 
+* units: the reference's model units, in which the inter-ocular distance is 89 units
+  (~63 mm, build/models/prepare_BFM.py:260-261), so that every unit-bearing constant of the
+  reference (the orthographic start sigma = 15, the initial light position and intensity, the
+  landmark initializer's slack) meets the scale it was tuned for; sizes below are quoted in
+  metres and converted with ``UNIT_M``;
 * geometry: ``V`` vertices on a face-like ellipsoid cap (half-axes a=0.08 m, b=0.10 m,
   depth c=0.05 m; the cap bulges toward the camera) with a nose, eye sockets and a brow
   ridge, Delaunay-triangulated and trimmed to ``T`` triangles by dropping the outermost ones;
@@ -53,12 +58,12 @@ KERNEL_SIGMA_TAPS = {  # 15-tap tables, src/lib/video_fitter.cu:53-56
            5.3990968e-02, 2.4197073e-01, 3.9894229e-01, 2.4197073e-01, 5.3990968e-02,
            4.4318484e-03, 1.3383022e-04, 1.4867194e-06, 6.0758834e-09, 9.1347208e-12],
 }
-# Initial light position and intensity of a video fit (src/lib/video_fitter.cu:115-116),
-# given there in model units where the inter-ocular distance is 89 units (~63 mm,
-# build/models/prepare_BFM.py:260-261). The synthetic model is in metres.
+# One model unit in metres: the inter-ocular distance is 89 units (~63 mm,
+# build/models/prepare_BFM.py:260-261). Initial light position and intensity of a video fit
+# (src/lib/video_fitter.cu:115-116) in those units; the intensity is held fixed by the video fit.
 UNIT_M = 0.063 / 89.0
-LAMBDA_INIT = (np.array([-7.3627, 51.1364, 100.1784]) * UNIT_M).astype(np.float32)
-L_INTENSITY = np.float32(0.5)   # metres^-1; intensity is held fixed by the video fit
+LAMBDA_INIT = np.array([-7.3627, 51.1364, 100.1784], dtype=np.float32)
+L_INTENSITY = np.float32(0.005)
 
 
 def _rng(config_id: int, stream: int) -> np.random.Generator:
@@ -241,7 +246,8 @@ def make_model(n_vertices: int, n_triangles: int, config_id: int = 0, n_expr: in
     else:
         tex = _face_albedo(rng, uv, u, v, beta, n_tex)
 
-    mean = np.stack([x, y, z]) + ident
+    mean = (np.stack([x, y, z]) + ident) / UNIT_M
+    E = E / UNIT_M
 
     # 51 landmarks by farthest-point sampling over the cap, starting at the centre.
     pts = np.c_[u, v]
@@ -309,7 +315,7 @@ def make_frames(model: Model, n_frames: int, config_id: int = 0, image_wh=(256, 
     """Per-frame cameras, poses, landmarks and initial states.
 
     ``box_range`` (px at the original resolution) draws the landmark-box size per frame and
-    sets tz from it; otherwise tz is fixed. ``ar1`` gives an AR(1) expression sequence
+    sets tz from it; otherwise tz is fixed (``tz`` in metres). ``ar1`` gives an AR(1) expression sequence
     (rho 0.95, unit marginal variance) and random-walk angles clamped to +-40 deg, else
     independent draws. Initial states stand in for the landmark initializer: ground truth
     state perturbed by ``init_pose_noise`` times (2 deg, 3 mm, 0.3 per expression),
@@ -364,7 +370,7 @@ def make_frames(model: Model, n_frames: int, config_id: int = 0, image_wh=(256, 
             box = rng_box.uniform(*box_range)
             tzf = focal * extent / box
         else:
-            tzf = tz
+            tzf = tz / UNIT_M
         # face centre somewhere inside the frame, away from the borders
         half = focal * extent / tzf * 0.75
         px = rng_box.uniform(min(half, W / 2), max(W - half, W / 2))
@@ -402,13 +408,13 @@ def make_frames(model: Model, n_frames: int, config_id: int = 0, image_wh=(256, 
         st_true[f, :K] = eps[f]
         st_true[f, K:K + 3] = tau
         st_true[f, K + 3:] = u
-        lam_true[f] = LAMBDA_INIT + rng.normal(0.0, 0.02, 3)
+        lam_true[f] = LAMBDA_INIT + rng.normal(0.0, 0.02, 3) / UNIT_M
         # Initial state: stands in for the landmark initializer. Perturb pose and
         # expressions, halving the perturbation until every landmark constraint is
         # strictly satisfied (the barrier needs a feasible start).
         scale = init_pose_noise
         dang = rng_noise.normal(0.0, 2.0, 3)
-        dtau = rng_noise.normal(0.0, 0.003, 3)
+        dtau = rng_noise.normal(0.0, 0.003, 3) / UNIT_M
         deps = rng_noise.normal(0.0, 0.3, K)
         fs = float(fs_all[f])
         for _ in range(12):

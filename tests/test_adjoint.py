@@ -133,7 +133,7 @@ def test_adjoint_against_the_references_gradient(tdi, synth, O, small_case):
     """The reference's gradient of its image term is its warp-only Jacobian contracted with the
     residual (no blur, shading or barycentric derivatives, approximate neighbours); here through
     the oracle pinned to the reference's kernels. It points the same way as the exact gradient
-    over the pose and within a stated angle overall."""
+    over the pose and overall: cosine at least 0.9 (0.96-0.99 measured on these frames)."""
     import torch
     ag = __import__("importlib").import_module("3di_b200.autograd")
     m, fr, om = small_case
@@ -149,4 +149,4 @@ def test_adjoint_against_the_references_gradient(tdi, synth, O, small_case):
         cos_all = gref @ gad / (np.linalg.norm(gref) * np.linalg.norm(gad))
         cos_pose = gref[K:] @ gad[K:] / (np.linalg.norm(gref[K:]) * np.linalg.norm(gad[K:]))
         print(f"frame {i}: cosine(reference J^T r, adjoint) all {cos_all:.4f}, pose {cos_pose:.4f}")
-        assert cos_pose >= 0.5 and cos_all >= 0.0
+        assert cos_pose >= 0.9 and cos_all >= 0.9

@@ -169,8 +169,10 @@ def test_tensor_core_normal_equations_within_fp32_accumulation_error(request, td
 def test_tensor_core_fit_reaches_the_exact_fits_objective(tdi, synth, O, small_case):
     """Fits with tensor-core normal equations follow different (rounding-level) search
     directions, so their iterates are not the oracle's; they must end at an objective within
-    0.5% of the exact fit's, with the same status flags, and with the pose (the well-determined
-    parameters) within 2% (median over frames; 10% at most) of the exact fit's."""
+    0.5% of the exact fit's, with the same status flags (apart from TDI_FLAG_FAIL, which marks a
+    shape fit of at most NITERS_SUCCESS outer iterations: a count the two can land on either
+    side of), and with the pose (the well-determined parameters) within 2% (median over frames;
+    10% at most) of the exact fit's."""
     m, fr, om = small_case
     model, batch, lam, L = _setup(tdi, small_case, synth)
     x0, lam0, rep0 = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(max_iters_rigid=10))
@@ -179,7 +181,7 @@ def test_tensor_core_fit_reaches_the_exact_fits_objective(tdi, synth, O, small_c
     K = m.n_expr
     pose_err = []
     for i in range(fr.n_frames):
-        assert rep1[i].flags == rep0[i].flags
+        assert (rep1[i].flags | tdi.FLAG_FAIL) == (rep0[i].flags | tdi.FLAG_FAIL)
         assert abs(rep1[i].objective - rep0[i].objective) <= 5e-3 * abs(rep0[i].objective)
         # pose (translation and rotation), the well-determined group, at parameter level
         pose_err.append(float((np.abs(x1[i, K:] - x0[i, K:]) / np.maximum(np.abs(x0[i, K:]), 1e-2)).max()))

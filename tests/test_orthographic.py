@@ -11,16 +11,17 @@ import pytest
 F32 = np.float32
 
 
-def _landmarks(O, p0L, rng, n):
-    """Scaled orthographic projections of the landmark points at random poses, with noise."""
+def _landmarks(O, p0L, rng, n, unit_m):
+    """Scaled orthographic projections of the landmark points at random poses, with noise:
+    600-1200 px per metre, offsets of about 1 cm (the model is in units of ``unit_m`` metres)."""
     xl, yl, us = [], [], []
     for _ in range(n):
         u = rng.normal(0, 0.15, 3).astype(F32)
         R, _ = O.rotation(u)
         rp = R.reshape(3, 3, order="F").astype(np.float64) @ p0L.astype(np.float64)
-        s = rng.uniform(600, 1200)
-        xl.append((s * (rp[0] + rng.normal(0, 0.01)) + 400 + rng.normal(0, 0.5, 51)).astype(F32))
-        yl.append((s * (rp[1] + rng.normal(0, 0.01)) + 300 + rng.normal(0, 0.5, 51)).astype(F32))
+        s = rng.uniform(600, 1200) * unit_m
+        xl.append((s * (rp[0] + rng.normal(0, 0.01) / unit_m) + 400 + rng.normal(0, 0.5, 51)).astype(F32))
+        yl.append((s * (rp[1] + rng.normal(0, 0.01) / unit_m) + 300 + rng.normal(0, 0.5, 51)).astype(F32))
         us.append(u)
     return np.array(xl), np.array(yl), np.array(us)
 
@@ -36,9 +37,9 @@ def _degrees(R):
     return [F32(float(F32(a * F32(180.0))) / math.pi) for a in video.euler_angles(R)]
 
 
-def test_oracle_fits_scaled_orthographic_landmarks(O, p0L):
+def test_oracle_fits_scaled_orthographic_landmarks(O, synth, p0L):
     rng = np.random.default_rng(7)
-    xl, yl, _ = _landmarks(O, p0L, rng, 12)
+    xl, yl, _ = _landmarks(O, p0L, rng, 12, synth.UNIT_M)
     fitted, rmss = 0, []
     for f in range(12):
         x, R, q = O.orthographic(xl[f], yl[f], p0L.reshape(-1))
@@ -57,10 +58,10 @@ def test_oracle_fits_scaled_orthographic_landmarks(O, p0L):
 
 
 @pytest.mark.gpu
-def test_device_matches_oracle(tdi, O, p0L):
+def test_device_matches_oracle(tdi, O, synth, p0L):
     tdi.require_gpu()
     rng = np.random.default_rng(11)
-    xl, yl, _ = _landmarks(O, p0L, rng, 37)
+    xl, yl, _ = _landmarks(O, p0L, rng, 37, synth.UNIT_M)
     x, ypr, it = tdi.orthographic_init(xl, yl, p0L)
     for f in range(37):
         ox, oR, oq = O.orthographic(xl[f], yl[f], p0L.reshape(-1))
