@@ -66,7 +66,7 @@ class FitConfig(C.Structure):
                 ("twostage_illum", C.c_int32), ("finetune", C.c_int32),
                 ("niters_success", C.c_int32), ("max_iters_lambda", C.c_int32),
                 ("ref_face_size", C.c_float), ("taps", C.c_float * 15), ("normal_eq", C.c_int32),
-                ("damping", C.c_float), ("host_rounds", C.c_int32)]
+                ("damping", C.c_float), ("host_rounds", C.c_int32), ("vertex_stage", C.c_int32)]
 
 
 class Report(C.Structure):
@@ -154,22 +154,27 @@ def require_gpu() -> None:
 
 
 NORMAL_EQ_EXACT, NORMAL_EQ_TENSOR = 0, 1
+VERTEX_EXACT, VERTEX_TENSOR = 0, 1
 
 
 def default_config(max_iters_rigid=100, max_iters_finetune=100, twostage_illum=0, finetune=0,
                    niters_success=6, max_iters_lambda=10000, ref_face_size=78.0,
-                   kernel_sigma=0.75, normal_eq=NORMAL_EQ_EXACT, damping=0.0, host_rounds=0) -> FitConfig:
+                   kernel_sigma=0.75, normal_eq=NORMAL_EQ_EXACT, damping=0.0, host_rounds=0,
+                   vertex_stage=VERTEX_EXACT) -> FitConfig:
     """Configuration keys of the reference's YAML config (src/lib/config.cu:350-541), plus
     ``normal_eq``: NORMAL_EQ_EXACT (FP64 in the oracle's order) or NORMAL_EQ_TENSOR
     (split-BF16 products on the tensor cores), and ``damping``: the lambda of the damped
     shape solve (H + lambda I) d = -g; 0 is the reference's undamped solve; ``host_rounds``: 1
-    launches every fitting round from the host instead of replaying CUDA graphs of rounds."""
+    launches every fitting round from the host instead of replaying CUDA graphs of rounds;
+    ``vertex_stage``: VERTEX_EXACT (FP32 fused multiply-add chains in the oracle's order) or
+    VERTEX_TENSOR (split-BF16 basis products on the tensor cores, FP32 accumulation)."""
     from . import synth
     c = FitConfig(max_iters_rigid, max_iters_finetune, twostage_illum, finetune, niters_success,
                   max_iters_lambda, ref_face_size)
     c.normal_eq = normal_eq
     c.damping = float(damping)
     c.host_rounds = int(host_rounds)
+    c.vertex_stage = int(vertex_stage)
     for i, t in enumerate(synth.KERNEL_SIGMA_TAPS[kernel_sigma]):
         c.taps[i] = t
     return c

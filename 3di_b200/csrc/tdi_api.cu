@@ -8,6 +8,7 @@
 // render the next outer iteration of the reference would redo at the same point.
 #include "tdi_kernels.cu"
 #include "tdi_normal_tc.cu"
+#include "tdi_vertex_tc.cu"
 #include "tdi_preprocess.cu"
 #include "tdi_orthographic.cu"
 #include "tdi_landmark.cu"
@@ -109,6 +110,9 @@ tdi_status check_cfg(const tdi_fit_config &c, const DModel &m)
         return fail(TDI_ERR_INVALID, "tensor-core normal equations take at most 121 expression components");
     if (c.normal_eq == 0 && m.KT + 1 > NE_P8)
         return fail(TDI_ERR_INVALID, "exact normal equations take at most 81 expression components");
+    if (c.vertex_stage != 0 && c.vertex_stage != 1) return fail(TDI_ERR_INVALID, "vertex_stage must be 0 or 1");
+    if (c.vertex_stage == 1 && !m.Etc)
+        return fail(TDI_ERR_INVALID, "the tensor-core vertex stage takes at most 80 expression components");
     return TDI_OK;
 }
 
@@ -126,6 +130,7 @@ Cfg to_cfg(const tdi_fit_config &c)
     r.normal_eq = c.normal_eq;
     r.damping = c.damping;
     r.host_rounds = c.host_rounds;
+    r.vertex_stage = c.vertex_stage;
     return r;
 }
 
@@ -275,6 +280,7 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_precheck, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<NE_GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<TC_MAXN / 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    TDI_CUDA(cudaFuncSetAttribute(k_vertex_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vc_smem(VC_MAXK)));
     done = true;
     return TDI_OK;
 }
@@ -293,6 +299,20 @@ dim3 vertex_grid(const DModel &m, int frames)
     const long ftiles = std::max(1, (frames + VT_F - 1) / VT_F);
     const long ntiles = (m.V + VT_V - 1) / VT_V;
     return dim3((unsigned)std::max(ftiles, std::min((long)VT_BLOCKS_PER_SM * sms, ftiles * ntiles)));
+}
+
+// Tensor-core vertex stage: one block per SM, split between frame tiles and vertex stripes.
+dim3 vertex_tc_grid(const DModel &m, int frames)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    const long ftiles = std::max(1, (frames + VC_F - 1) / VC_F);
+    const long ntiles = (m.V + VC_V - 1) / VC_V;
+    return dim3((unsigned)std::max(ftiles, std::min((long)sms, ftiles * ntiles)));
 }
 
 // Blocks per frame of the depth pass: 16, or more when few frames run, so that a short
@@ -402,7 +422,11 @@ tdi_status geometry(const Launch &L, const Cfg &c, int stage)
     TDI_TRY(launch(L.bt, 0, k_precheck, dim3((L.A() + PC_WARPS - 1) / PC_WARPS), dim3(PC_WARPS * 32),
                    precheck_smem(L.m.K, L.m.KP), L.s, L.m, L.b, c, stage));
     TDI_TRY(launch(L.bt, 0, k_compact_render, dim3(1), dim3(1024), 0, L.s, L.b));
-    TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, VT_WARPS + 1), L.smem_vertex(), L.s, L.m, L.b));
+    if (c.vertex_stage == 1)
+        TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex_tc, vertex_tc_grid(L.m, L.A()), dim3(VC_THREADS), vc_smem(L.m.K),
+                       L.s, L.m, L.b, reinterpret_cast<const __nv_bfloat16 *>(L.m.Etc)));
+    else
+        TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, VT_WARPS + 1), L.smem_vertex(), L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(raster_blocks(L.A()), L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RESOLVE, k_raster_resolve, dim3(L.A()), dim3(RR_THREADS), 0, L.s, L.m, L.b));
     return TDI_OK;
@@ -702,6 +726,16 @@ tdi_status tdi_model_create(const tdi_model_desc *desc, tdi_model **out)
         cudaMemcpy(tlo4, tlo4_h.data(), sizeof(int4) * T, cudaMemcpyHostToDevice) != cudaSuccess)
         return cleanup(fail(TDI_ERR_CUDA, "model upload failed"));
     d.mean = mean; d.E = E; d.tex = tex; d.tl = tl; d.lis = lis; d.eps_b = epsb; d.tri_order = order; d.tlo = tlo; d.tl4 = tl4; d.tlo4 = tlo4;
+    if (K <= VC_MAXK) {
+        // the basis split into BF16 pieces once, in the tensor-core vertex stage's tile layout
+        const int ntiles = (V + VC_V - 1) / VC_V;
+        uint8_t *etc = nullptr;
+        if ((st = dalloc(m->allocs, &etc, (size_t)ntiles * vc_tile_bytes(K)))) return cleanup(st);
+        k_split_basis<<<1024, 256>>>(d, ntiles, reinterpret_cast<__nv_bfloat16 *>(etc));
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+            return cleanup(fail(TDI_ERR_CUDA, "basis split failed"));
+        d.Etc = etc;
+    }
     *out = m;
     return TDI_OK;
 }

@@ -78,6 +78,7 @@ struct Cfg {
     int32_t normal_eq;       // 0: FP64 in the oracle's order; 1: split-BF16 tensor cores
     float damping;           // lambda of the damped shape solve (H + lambda I), 0 = undamped
     int32_t host_rounds;     // 1: host-driven rounds instead of replayed graphs
+    int32_t vertex_stage;    // 0: FP32 fused multiply-add chains; 1: split-BF16 tensor cores
 };
 
 // Device view of the model.
@@ -96,6 +97,8 @@ struct DModel {
     const int32_t *tlo;      // [3][T] corner slots of the triangles in tri_order
     const int4 *tl4;         // [T] corner slots (b, c, a, 0): one 16-byte gather per triangle
     const int4 *tlo4;        // [T] in tri_order: corner slots and the triangle id (b, c, a, tri)
+    const void *Etc;         // the basis split into BF16 pieces in the tensor-core vertex stage's
+                             // tile layout (null when K is above that stage's limit)
 };
 
 // Device view of a batch of frames and its working set.

@@ -6,7 +6,9 @@ reference's full-size model (53,490 vertices, 106,466 triangles, 79 expression c
 a batch of video frames (AR(1) expressions, random-walk head pose, face boxes 120-600 px in
 1080p) rescaled to the reference's 256x256 crop, fitted per frame as
 VideoFitter::fit_to_video_frame does after its landmark initialisation: light fit, then the
-log-barrier Gauss-Newton shape fit (pose + 79 expressions) capped at 20 outer iterations.
+log-barrier Gauss-Newton shape fit (pose + 79 expressions) capped at 20 outer iterations. The
+fits start from the device landmark initializer's states (tdi_batch_landmark_init, run once
+before timing; its own rate is the ``landmark_init`` field).
 
 One step = one fit of the whole batch. ``value`` times ``tdi_batch_fit`` with every input
 resident in device memory; ``e2e`` times ``tdi_fit_frames`` from pinned host buffers
@@ -14,8 +16,8 @@ resident in device memory; ``e2e`` times ``tdi_fit_frames`` from pinned host buf
 Inputs (256 MB of target crops for 1,024 frames) exceed the 126 MB L2 between steps.
 
 ``--impl reference`` times the CPU restatement of the same path (oracle/, OpenMP over frames,
-all host threads) on a bounded sample of the same frames: 3DI cannot be built here (it needs
-OpenCV) and has no CPU path of its own.
+all host threads) on a bounded sample of the same frames: 3DI's path is CUDA-only and has no
+CPU implementation of its own (its kernels are built from its sources for parity tests only).
 """
 from __future__ import annotations
 
@@ -218,6 +220,10 @@ def reference_arm(args, world, rank):
     n = args.cpu_frames
     m, fr = make_workload(synth, n)
     render_targets_cpu(O, synth, m, fr)
+    om = O.Model(m)
+    fs = O.FrameSet(fr)
+    p0L = landmark_points(m)
+    fr.state_init = np.stack([O.landmark_init(om, fs, i, p0L)[0] for i in range(n)])
     threads = O.max_threads()
     rates = []
     for _ in range(args.warmup if args.warmup < 1 else 1):
@@ -233,12 +239,18 @@ def reference_arm(args, world, rank):
         "config": {"workload": WORKLOAD, "frames_per_step": n, "max_outer_iters": MAX_ITERS,
                    "l2": "inputs larger than L2 are not applicable on the CPU"},
         "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} frames of {WORKLOAD}, FP32 CPU restatement (oracle/), "
-                                   "3DI itself needs OpenCV and cannot be built"},
+                         "sample": f"{n} frames of {WORKLOAD} from the landmark initializer's states, "
+                                   "FP32 CPU restatement (oracle/); 3DI's path is CUDA-only, it has no "
+                                   "CPU implementation"},
         "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def landmark_points(m):
+    """The landmark vertices of the subject's shape, [3][51] (the reference's p0L_mat.dat)."""
+    return np.ascontiguousarray(m.mean[:, m.lis].astype(np.float32))
 
 
 def render_targets_cpu(O, synth, m, fr):
@@ -268,12 +280,12 @@ def fit_timed(batch, cfg, fr, lam0, L, steps, barrier):
     return total
 
 
-def kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl):
+def kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl, names=None):
     """Every major kernel timed live with CUDA events on its stream, one untimed fit per kernel
     (tdi_batch_profile): launches, device time, frames processed, share of the kernels' sum,
     and its roofline against its algorithmic bytes (or flops)."""
     rows = {}
-    for name in KERNELS:
+    for name in (names or KERNELS):
         batch.set_state(fr.state_init, lam0, L)
         batch.profile(name)
         batch.fit(cfg)
@@ -282,7 +294,7 @@ def kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl):
         rows[name] = {"launches": n, "ms": ms, "frames": frames}
     total = sum(r["ms"] for r in rows.values())
     for name, r in rows.items():
-        r["share"] = r["ms"] / total if total else None
+        r["share"] = r["ms"] / total if total and names is None else None
         r["us_per_frame"] = 1000.0 * r["ms"] / r["frames"] if r["frames"] else None
         per_frame, per_launch = algorithmic_bytes(name, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
         if per_frame is not None and r["launches"]:
@@ -291,6 +303,10 @@ def kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl):
             bpl = per_frame * fpl + per_launch
             r["hbm_gbs"] = bpl / avg_s / 1e9
             r["hbm_frac"] = r["hbm_gbs"] / hbm
+        if name == "vertex" and cfg.vertex_stage == 1 and r["launches"]:
+            r["tflops_tensor"] = 6 * vertex_flops_per_frame(m.n_vertices, m.n_expr) * r["frames"] / (r["ms"] / 1000.0) / 1e12
+            r["tflops_tensor_note"] = "six split-BF16 products per FP32 product, against the measured bf16 peak"
+            r["tflops_tensor_frac"] = r["tflops_tensor"] / tfl
         if name == "normal_eq" and r["launches"]:
             fl = normal_eq_flops_per_frame(m.n_expr, n_frag) * r["frames"] / (r["ms"] / 1000.0) / 1e12
             r["tflops"] = fl
@@ -359,6 +375,11 @@ def main():
     img, _ = batch.render()
     fr.target = synth.add_noise(img, 0.02, 3 + rank)
     batch.set_frames(fr)
+    # every fit starts from the device landmark initializer's output (computed once here; its
+    # own rate is measured below)
+    p0L = landmark_points(m)
+    lm_ok, _, lm_it = batch.landmark_init(p0L)
+    fr.state_init = batch.get_state()[0].copy()
     lam0 = np.tile(synth.LAMBDA_INIT, (F, 1)).astype(np.float32)
     neq = tdi.NORMAL_EQ_TENSOR if args.normal_eq == "tensor" else tdi.NORMAL_EQ_EXACT
     cfg = tdi.default_config(max_iters_rigid=MAX_ITERS, normal_eq=neq)
@@ -419,6 +440,13 @@ def main():
     batch.fit(cfg_o)
     other_ms = fit_timed(batch, cfg_o, fr, lam0, L, args.steps, barrier)
     xo_gpu, _, rep_o = batch.get_state()
+    # both contractions on the tensor cores: the vertex stage and the normal equations
+    cfg_t = tdi.default_config(max_iters_rigid=MAX_ITERS, normal_eq=tdi.NORMAL_EQ_TENSOR,
+                               vertex_stage=tdi.VERTEX_TENSOR)
+    batch.set_state(fr.state_init, lam0, L)
+    batch.fit(cfg_t)
+    tensor_all_ms = fit_timed(batch, cfg_t, fr, lam0, L, args.steps, barrier)
+    _, _, rep_t = batch.get_state()
     # the reference's cfg1 stage sequence: two-stage illumination and the expression finetune
     cfg1 = tdi.default_config(max_iters_rigid=MAX_ITERS, max_iters_finetune=MAX_ITERS, twostage_illum=1,
                               finetune=1, normal_eq=neq)
@@ -426,11 +454,25 @@ def main():
     batch.fit(cfg1)
     cfg1_ms = fit_timed(batch, cfg1, fr, lam0, L, args.steps, barrier)
     _, _, rep1 = batch.get_state()
+    # the landmark initialisation of the same frames (orthographic fit + barrier method)
+    lm_ms = 0.0
+    for _ in range(args.steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.landmark_init(p0L)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        lm_ms += e0.elapsed_time(e1)
     h2d = sum(h[k].numel() * h[k].element_size() for k in ("t", "xl", "yl", "b", "fs", "cam", "o", "x", "lam", "L"))
     d2h = F * (m.n_expr + 6) * 4 + F * 3 * 4 + F * C.sizeof(tdi.Report)
 
     # max over ranks
-    total_ms, e2e_ms, other_ms, cfg1_ms = max_over_ranks([total_ms, e2e_ms, other_ms, cfg1_ms], world, device="cuda")
+    total_ms, e2e_ms, other_ms, cfg1_ms, lm_ms, tensor_all_ms = max_over_ranks(
+        [total_ms, e2e_ms, other_ms, cfg1_ms, lm_ms, tensor_all_ms], world, device="cuda")
     frames_all = F * world * args.steps
     value = job_rate(F, world, args.steps, total_ms)
     e2e = job_rate(F, world, args.steps, e2e_ms)
@@ -438,6 +480,7 @@ def main():
     # per-kernel live timing (untimed fits) and the roofline of the largest-share kernel
     hbm, tfl, peak_kind = measured_peaks()
     kt = kernel_table(batch, cfg, fr, lam0, L, m, n_frag, hbm, tfl)
+    kt_t = kernel_table(batch, cfg_t, fr, lam0, L, m, n_frag, hbm, tfl, names=("vertex", "normal_eq"))
     top = max((k for k in kt if "hbm_gbs" in kt[k]), key=lambda k: kt[k]["ms"])
     per_frame, per_launch = algorithmic_bytes(top, m.n_vertices, m.n_triangles, m.n_expr, n_frag)
     tr_ = kt[top]
@@ -477,14 +520,26 @@ def main():
                             other: {"value": frames_all / (other_ms / 1000.0), "ms_per_step": other_ms / args.steps,
                                     "mean_renders": float(np.mean([r.renders for r in rep_o])),
                                     "failed": int(sum(1 for r in rep_o if r.flags & tdi.FLAG_FAIL))},
+                            "tensor_vertex_and_normal_eq": {
+                                "value": frames_all / (tensor_all_ms / 1000.0), "ms_per_step": tensor_all_ms / args.steps,
+                                "mean_renders": float(np.mean([r.renders for r in rep_t])),
+                                "failed": int(sum(1 for r in rep_t if r.flags & tdi.FLAG_FAIL)),
+                                "kernels": kt_t},
                             "note": "exact: FP64 normal equations in the oracle's order (bit-identical fits); "
-                                    "tensor: split-BF16 tcgen05 products, FP32 chunk accumulation"},
+                                    "tensor: split-BF16 tcgen05 products, FP32 chunk accumulation; "
+                                    "tensor_vertex_and_normal_eq: the vertex stage's basis products on tcgen05 "
+                                    "as well (split BF16, FP32 accumulation)"},
         "stage_sequences": {"light_shape": {"value": value, "note": "light fit + shape fit (one face scale)"},
                             "cfg1": {"value": frames_all / (cfg1_ms / 1000.0), "ms_per_step": cfg1_ms / args.steps,
                                      "mean_iters_finetune": float(np.mean([r.iters_finetune for r in rep1])),
                                      "note": "light, shape, two-stage illumination (2 more light + shape fits) "
                                              "and the expression finetune, as the reference's cfg1 runs each "
                                              "face scale"}},
+        "landmark_init": {"value": frames_all / (lm_ms / 1000.0), "unit": "frames/s",
+                          "succeeded": int(lm_ok.sum()), "frames": F,
+                          "mean_newton_iters": float(np.mean(lm_it)),
+                          "note": "tdi_batch_landmark_init: orthographic fit, mirrored refit, barrier method "
+                                  "with slack; the fits above start from its output"},
         "clocks": clk,
         "fit": {"mean_iters_rigid": float(np.mean([r.iters_rigid for r in rep])),
                 "mean_iters_lambda": float(np.mean([r.iters_lambda for r in rep])),
@@ -534,16 +589,23 @@ def main():
                     key = "vs_" + ("fp32" if kind == "f32" else "fp64") + "_oracle"
                     rel = np.abs(xg[:n] - ox) / np.maximum(np.abs(ox), 1e-2)
                     K = m.n_expr
+                    # pose: translation relative to the depth, rotation vector in radians
+                    dt = np.abs(xg[:n, K:K + 3] - ox[:, K:K + 3]).max(axis=1) / np.abs(ox[:, K + 2])
+                    du = np.abs(xg[:n, K + 3:K + 6] - ox[:, K + 3:K + 6]).max(axis=1)
                     errs[mode][key] = {
                         "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
-                        "pose_median_rel": float(np.median(rel[:, K:])), "pose_max_rel": float(rel[:, K:].max()),
+                        "expr_median_rel": float(np.median(rel[:, :K])),
+                        "tau_over_depth_median": float(np.median(dt)), "tau_over_depth_max": float(dt.max()),
+                        "rotation_rad_median": float(np.median(du)), "rotation_rad_max": float(du.max()),
                         "frames_within_1e-5": int(np.sum(rel.max(axis=1) <= 1e-5))}
                     if mode == args.normal_eq:
                         errs[mode][key]["light_max_rel"] = float(
                             (np.abs(lamf[:n] - ol) / np.maximum(np.abs(ol), 1e-6)).max())
             line["param_err"] = {"frames": n, **errs[args.normal_eq], other: errs[other],
                                  "definition": "|x_gpu - x_oracle| / max(|x_oracle|, 1e-2) over pose and expressions "
-                                               "after the whole fit; light: |lam_gpu - lam_oracle| / |lam_oracle|"}
+                                               "after the whole fit; tau_over_depth: |tau_gpu - tau_oracle|_inf / "
+                                               "|tau_z|; rotation_rad: |u_gpu - u_oracle|_inf; light: "
+                                               "|lam_gpu - lam_oracle| / |lam_oracle|"}
             # every output of one Gauss-Newton step against the FP64 oracle, both modes
             line["step_err"] = {
                 "frames": n,

@@ -128,6 +128,11 @@ typedef struct {
                                   * CUDA graphs of 16 rounds, the host reading the active-frame count
                                   * once per replay; 1: the host launches every round and reads the
                                   * count after each (the same kernels and results). */
+    int32_t vertex_stage;        /* basis x coefficients of the vertex stage (renderer.cu:806-861):
+                                  * 0 = FP32 fused multiply-add chains in the oracle's order
+                                  * (bit-exact); 1 = split-BF16 products on the tensor cores with
+                                  * FP32 accumulation (at most 80 expression components). Applies
+                                  * to tdi_batch_fit and tdi_batch_evaluate. */
 } tdi_fit_config;
 
 typedef struct {

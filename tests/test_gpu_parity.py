@@ -21,6 +21,14 @@ def _setup(tdi, case, synth):
     return model, batch, lam, L
 
 
+def _pose_difference(x, x_ref, K):
+    """max(|tau - tau_ref|_inf / |tau_z ref|, |u - u_ref|_inf in radians): translation relative to
+    the depth, rotation absolute (relative differences of near-zero components mean nothing)."""
+    dt = np.abs(x[K:K + 3] - x_ref[K:K + 3]).max() / abs(float(x_ref[K + 2]))
+    du = np.abs(x[K + 3:K + 6] - x_ref[K + 3:K + 6]).max()
+    return float(max(dt, du))
+
+
 def _bits(a):
     return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
 
@@ -171,8 +179,9 @@ def test_tensor_core_fit_reaches_the_exact_fits_objective(tdi, synth, O, small_c
     directions, so their iterates are not the oracle's; they must end at an objective within
     0.5% of the exact fit's, with the same status flags (apart from TDI_FLAG_FAIL, which marks a
     shape fit of at most NITERS_SUCCESS outer iterations: a count the two can land on either
-    side of), and with the pose (the well-determined parameters) within 2% (median over frames;
-    10% at most) of the exact fit's."""
+    side of), and with the pose (the well-determined parameters) close to the exact fit's: the
+    larger of the translation difference relative to the depth and the rotation-vector difference
+    in radians at most 1e-2 (median over frames; 5e-2 at most)."""
     m, fr, om = small_case
     model, batch, lam, L = _setup(tdi, small_case, synth)
     x0, lam0, rep0 = batch.fit_frames(fr, fr.state_init, lam, L, tdi.default_config(max_iters_rigid=10))
@@ -184,9 +193,9 @@ def test_tensor_core_fit_reaches_the_exact_fits_objective(tdi, synth, O, small_c
         assert (rep1[i].flags | tdi.FLAG_FAIL) == (rep0[i].flags | tdi.FLAG_FAIL)
         assert abs(rep1[i].objective - rep0[i].objective) <= 5e-3 * abs(rep0[i].objective)
         # pose (translation and rotation), the well-determined group, at parameter level
-        pose_err.append(float((np.abs(x1[i, K:] - x0[i, K:]) / np.maximum(np.abs(x0[i, K:]), 1e-2)).max()))
+        pose_err.append(_pose_difference(x1[i], x0[i], K))
     print("tensor vs exact fit, pose relative difference per frame:", pose_err)
-    assert np.median(pose_err) <= 2e-2 and max(pose_err) <= 1e-1
+    assert np.median(pose_err) <= 1e-2 and max(pose_err) <= 5e-2
 
 
 @pytest.mark.parametrize("case_name", ["small_case", "full_case"])

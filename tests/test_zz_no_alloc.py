@@ -159,3 +159,39 @@ def test_noalloc_raster_rejects_meshes_above_its_fixed_size():
     dummy = C.c_void_p(16)   # never dereferenced: the size check comes first
     st = lib.tdi_raster_noalloc(dummy, dummy, dummy, dummy, 10, 131073, 0, 0, dummy, 16, dummy, dummy, None)
     assert st == 4 and b"131072" in lib.tdi_last_error()
+
+
+def test_noalloc_raster_equals_oracle_on_the_full_size_mesh(O, full_case):
+    """The 53,490-vertex / 106,466-triangle mesh (the size the fixed 131,072-triangle working
+    array is for), at the true and the initial states of each frame: fragments bit for bit the
+    oracle's (count, slot order, pixels, triangles, barycentric bits, owners)."""
+    tdi = importlib.import_module("3di_b200")
+    tdi.require_gpu()
+    import torch
+    m, fr, om = full_case
+    lib = tdi.load_library()
+    dev = torch.device("cuda", 0)
+    tl = torch.from_numpy(np.ascontiguousarray(m.tl, dtype=np.int32)).to(dev)
+    cap = 4 * m.n_triangles
+    out = torch.zeros(cap * 4, dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    flags = torch.zeros(1, dtype=torch.int32, device=dev)
+    for i in range(fr.n_frames):
+        for state in (fr.state_true[i], fr.state_init[i]):
+            geo, ok = O.vertex_stage(om, state, fr.cam[i])
+            xp, yp, zc = geo[6], geo[7], geo[5]
+            x0, y0 = (int(v) for v in fr.x0y0[i])
+            ref = O.raster(om, xp, yp, zc, x0, y0)
+            d = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev) for a in (xp, yp, zc)]
+            st = _noalloc(lib, d, tl, m.n_vertices, m.n_triangles, x0, y0, out, cap, count, flags)
+            assert st == 0, lib.tdi_last_error()
+            torch.cuda.synchronize()
+            n = int(count.item())
+            assert n == ref["N"] and n > 1000
+            got = out[:4 * n].cpu().numpy().reshape(n, 4)
+            po = got[:, 0].view(np.uint32)
+            assert np.array_equal((po & 0xFFFF).astype(np.uint16), ref["pix"])
+            assert np.array_equal((po >> 31).astype(np.uint8), ref["owner"])
+            assert np.array_equal(got[:, 1], ref["tri"])
+            assert np.array_equal(got[:, 2].view(np.uint32), ref["al"].view(np.uint32))
+            assert np.array_equal(got[:, 3].view(np.uint32), ref["be"].view(np.uint32))
