@@ -2062,16 +2062,20 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
 // FP64 Cholesky solve (solver.h:70-105, cuSOLVER DPOTRF/DPOTRS in the reference) of the shape
 // system, one block per frame, then the first trial of the line search.
 //
+// Arithmetic (shared with the oracle's solve_shape): pivots l_jj = sqrt(s_j) with reciprocal
+// r_j = 1 / l_jj; L(i,j) = t_ij * r_j, where t_ij is a_ij minus L(i,k) L(j,k) for k = 0, 1, ...
+// in increasing k (each product and difference rounded); forward y_i = (g_i - sum_k L(i,k) y_k)
+// * r_i with terms in increasing k; back x_i = (y_i - sum_k L(k,i) x_k) * r_i with terms in
+// decreasing k. (cuSOLVER's order is the library's; the reciprocal is one rounding per column.)
+//
 // The lower triangle is held in registers: thread (tr, tc) = (tid % 16, tid / 16) owns the
-// entries (i, l) with i = tr + 16a, l = tc + 16b, i >= l. Step j: the pivot's owner takes the
-// square root; threads j+1..n-1 each divide one entry of column j (its owner left the
-// updated value in shared memory during the previous step); every thread then subtracts
-// L(i,j) L(l,j) from its entries right of column j. Each entry so receives its updates in
-// increasing j, the same sequence of subtractions as the oracle's left-looking dot products.
-// The forward substitution rides along (thread j divides y_j at step j, threads i > j then
-// update y_i, terms in increasing k); the back substitution runs by columns with terms in
-// decreasing k (the oracle's order), y_i held by thread i. Two barriers per factor step, one
-// per back step.
+// entries (i, l) with i = tr + 16a, l = tc + 16b, i >= l. Step j: every thread reads column j
+// as its owners left it in shared memory (pivot included), forms l_jj and r_j itself (the same
+// correctly rounded values everywhere) and the scaled entries it needs, and subtracts
+// L(i,j) L(l,j) from its entries right of column j; the owners of column j + 1 then store it
+// for the next step. Each entry so receives its updates in increasing j, the sequence of the
+// oracle's left-looking dot products. One barrier per step; the two substitutions run in one
+// warp, four rows per lane, the newly known value broadcast by shuffle.
 
 constexpr int SV_THREADS = 256;
 constexpr int SV_MAXN = 128;
@@ -2081,18 +2085,38 @@ __host__ __device__ __forceinline__ size_t solve_smem(int n)
     return ((size_t)n * n + 4 * SV_MAXN + 2) * sizeof(double);
 }
 
+// One substitution pass of the warp: rows i = lane + 32 q (q < 4) start from t[q]; for each
+// step k (ascending when fwd, descending otherwise) the owner of row k forms x_k = t_k * r_k,
+// every row i after k in that order subtracts coef(i, k) x_k. Results in out[].
+template <bool FWD>
+__device__ __forceinline__ void sv_substitute(int n, double (&t)[4], const double *Lf, const double *rv, double *out)
+{
+    const int lane = threadIdx.x & 31;
+    for (int s = 0; s < n; ++s) {
+        const int k = FWD ? s : n - 1 - s;
+        const int q = k >> 5;
+        const double tk = q == 0 ? t[0] : q == 1 ? t[1] : q == 2 ? t[2] : t[3];
+        const double xk = __shfl_sync(0xffffffffu, tk, k & 31) * rv[k];
+        if (lane == 0) out[k] = xk;
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+            const int i = lane + 32 * qq;
+            // forward: L(i,k) for i > k (column k); back: L(k,i) for i < k (column i)
+            if (FWD ? (i > k && i < n) : (i < k)) t[qq] -= (FWD ? Lf[(size_t)k * n + i] : Lf[(size_t)i * n + k]) * xk;
+        }
+    }
+}
+
 template <int RB>
 __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, const Cfg &c, int stage, int f,
                                             FrameCtl &ctl, double *sm)
 {
     const int n = m.KT, KTP = m.KTP, K = m.K;
     const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
-    double *Lf = sm;                     // [n][n] column-major: the factor, for the back steps
-    double *raw = Lf + (size_t)n * n;    // column j before its scaling
-    double *col = raw + SV_MAXN;         // column j after its scaling
-    double *yv = col + SV_MAXN;          // forward results y_j / L(j,j)
-    double *yb = yv + SV_MAXN;           // back results
-    double *piv = yb + SV_MAXN;          // [0] pivot, [1] failure flag
+    double *Lf = sm;                     // [n][n] column-major: the factor, for the substitutions
+    double *raw = Lf + (size_t)n * n;    // [2][SV_MAXN] column j before its scaling (by step parity)
+    double *rv = raw + 2 * SV_MAXN;      // [SV_MAXN] reciprocal pivots
+    double *yv = rv + SV_MAXN;           // [SV_MAXN] forward, then back results
     const float *H = b.H + (size_t)f * KTP * KTP;
     const float *gv = b.g + (size_t)f * KTP;
     double v[RB][RB];
@@ -2105,28 +2129,15 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
             v[a][bb] = (i < n && l < n && i >= l) ? (double)H[(size_t)l * KTP + i] : 0.0;
             if (i == l && i < n) v[a][bb] += lam_d;
         }
-    double y = tid < n ? (double)gv[tid] : 0.0;
-    if (tid == 0) piv[1] = 0.0;
-    // column 0 before scaling
+    // column 0 before scaling, pivot included
 #pragma unroll
     for (int a = 0; a < RB; ++a)
         if (tc == 0 && tr + 16 * a < n) raw[tr + 16 * a] = v[a][0];
     __syncthreads();
     for (int j = 0; j < n; ++j) {
-        const int jt = j & 15, jb = j >> 4;
-        if (tr == jt && tc == jt) {                  // the pivot's owner
-#pragma unroll
-            for (int a = 0; a < RB; ++a)
-                if (a == jb) {
-                    const double s = v[a][a];
-                    if (!(s > 0.0)) piv[1] = 1.0;
-                    const double ljj = sqrt(s);
-                    piv[0] = ljj;
-                    Lf[(size_t)j * n + j] = ljj;
-                }
-        }
-        __syncthreads();
-        if (piv[1] != 0.0) {                         // block-uniform: the pivot was not positive
+        const double *rj = raw + (j & 1) * SV_MAXN;
+        const double sj = rj[j];
+        if (!(sj > 0.0)) {                           // block-uniform: every thread read the same pivot
             float *d = b.d + (size_t)f * KTP;
             for (int i = tid; i < n; i += SV_THREADS) d[i] = __int_as_float(0x7fc00000);
             if (tid == 0) {
@@ -2135,21 +2146,16 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
             }
             return;
         }
-        const double ljj = piv[0];
-        if (tid > j && tid < n) {
-            const double lij = raw[tid] / ljj;
-            col[tid] = lij;
-            Lf[(size_t)j * n + tid] = lij;
-        }
-        if (tid == j) { y = y / ljj; yv[j] = y; }
-        __syncthreads();
+        const double ljj = sqrt(sj), r = 1.0 / ljj;
+        if (tid == 0) { Lf[(size_t)j * n + j] = ljj; rv[j] = r; }
+        if (tid > j && tid < n) Lf[(size_t)j * n + tid] = rj[tid] * r;
         // trailing update of the owned entries right of column j
         double ci[RB], cl[RB];
 #pragma unroll
         for (int a = 0; a < RB; ++a) {
             const int i = tr + 16 * a, l = tc + 16 * a;
-            ci[a] = (i > j && i < n) ? col[i] : 0.0;
-            cl[a] = (l > j && l < n) ? col[l] : 0.0;
+            ci[a] = (i > j && i < n) ? rj[i] * r : 0.0;
+            cl[a] = (l > j && l < n) ? rj[l] * r : 0.0;
         }
 #pragma unroll
         for (int a = 0; a < RB; ++a)
@@ -2158,27 +2164,41 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
                 const int i = tr + 16 * a, l = tc + 16 * bb;
                 if (l > j && i >= l && i < n) v[a][bb] -= ci[a] * cl[bb];
             }
-        if (tid > j && tid < n) y -= col[tid] * yv[j];
-        // the next column before its scaling
+        // the next column before its scaling, pivot included
         const int jn = j + 1;
         if (jn < n && tc == (jn & 15)) {
+            double *rn = raw + (jn & 1) * SV_MAXN;
 #pragma unroll
             for (int a = 0; a < RB; ++a)
 #pragma unroll
                 for (int bb = 0; bb < RB; ++bb)
                     if (bb == (jn >> 4)) {
                         const int i = tr + 16 * a;
-                        if (i > jn && i < n) raw[i] = v[a][bb];
+                        if (i >= jn && i < n) rn[i] = v[a][bb];
                     }
         }
+        __syncthreads();
+    }
+    // forward and back substitution in one warp
+    if (tid < 32) {
+        double t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = tid + 32 * q;
+            t[q] = i < n ? (double)gv[i] : 0.0;
+        }
+        sv_substitute<true>(n, t, Lf, rv, yv);
+        // y_i = t_i r_i: the value the owner of row i broadcast at step i
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = tid + 32 * q;
+            t[q] = i < n ? t[q] * rv[i] : 0.0;
+        }
+        __syncwarp();
+        sv_substitute<false>(n, t, Lf, rv, yv);
     }
     __syncthreads();
-    // back substitution: y_k / L(k,k), then y_i -= L(k,i) y_k for i < k
-    for (int k = n - 1; k >= 0; --k) {
-        if (tid == k) { y = y / Lf[(size_t)k * n + k]; yb[k] = y; }
-        __syncthreads();
-        if (tid < k) y -= Lf[(size_t)tid * n + k] * yb[k];
-    }
+    const double y = tid < n ? yv[tid] : 0.0;
     // direction, its slope and the first trial point
     float *d = b.d + (size_t)f * KTP;
     float *dsm = reinterpret_cast<float *>(raw);

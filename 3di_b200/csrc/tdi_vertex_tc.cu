@@ -13,11 +13,13 @@
 // One block per SM, persistent over vertex tiles of 32 vertices for a tile of 128 frames:
 // the tensor-core tile is M = 128 rows (x, y, z rows of the 32 vertices and 32 rows that are
 // never read) by N = 128 frames by K (the coefficients, padded to a multiple of 16).
-//   warp 8, one thread: bulk copies of the pre-split basis tiles (46 KB) into two buffers, the
-//     30 MMAs of a tile into one of two tensor-memory accumulators, commits;
-//   warps 0-7: the epilogue -- tensor memory -> shared memory (x, y, z of each vertex and
-//     frame), then mean + product, rotation, translation and projection per vertex and frame,
-//     written as the exact stage writes them (geometry and projection records).
+//   warp 16, one thread: bulk copies of the pre-split basis tiles (46 KB) into two buffers,
+//     the 30 MMAs of a tile into one of two tensor-memory accumulators, commits;
+//   warps 0-15: the epilogue -- tensor memory -> shared memory (x, y, z of each vertex and
+//     frame; warp w reads lane group w % 4, frame quarter w / 4), then mean + product,
+//     rotation, translation and projection per vertex and frame, written as the exact stage
+//     writes them (geometry and projection records). Sixteen warps keep enough stores in
+//     flight; the stage is bound by those stores.
 // The copy of tile j + 2, the MMAs of tile j + 1 and the epilogue of tile j overlap. Every
 // mbarrier wait gives up after about a second: the block sets the batch's error word, waits
 // (again bounded) for its copies and MMAs in flight and frees its tensor memory.
@@ -27,7 +29,7 @@ namespace tdi {
 constexpr int VC_V = 32;                          // vertices per tile
 constexpr int VC_F = 128;                         // frames per block (the MMA's N)
 constexpr int VC_M = 128;                         // accumulator rows (x, y, z rows + 32 unused)
-constexpr int VC_EPI_WARPS = 8;
+constexpr int VC_EPI_WARPS = 16;                  // four per tensor-memory lane group
 constexpr int VC_THREADS = (VC_EPI_WARPS + 1) * 32;
 constexpr int VC_MAXK = 80;                       // coefficients supported (K padded to 16)
 constexpr int VC_ROWGROUPS = 3 * VC_V / 8;        // 12 groups of 8 rows hold data
@@ -222,7 +224,7 @@ __global__ void __launch_bounds__(VC_THREADS, 1) k_vertex_tc(DModel m, DBatch b,
             }
         }
     } else {
-        const int lg = warp & 3, half = warp >> 2;         // tensor-memory lane group, frame half
+        const int lg = warp & 3, qt = warp >> 2;           // tensor-memory lane group, frame quarter
         for (int j = 0;; ++j) {
             const int t = gy + j * groups;
             if (t >= ntiles) break;
@@ -240,14 +242,15 @@ __global__ void __launch_bounds__(VC_THREADS, 1) k_vertex_tc(DModel m, DBatch b,
             if (s_epi_abort) break;
             tc_fence_after();
             if (lg < 3) {
-                // rows 32 lg + lane: coordinate lg of vertex `lane`, frames of this half
-                const uint32_t taddr = tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)(buf * VC_F + half * (VC_F / 2));
+                // rows 32 lg + lane: coordinate lg of vertex `lane`, frames of this quarter
+                constexpr int QF = VC_F / 4;
+                const uint32_t taddr = tmem + ((uint32_t)(32 * lg) << 16) + (uint32_t)(buf * VC_F + qt * QF);
 #pragma unroll
-                for (int cb = 0; cb < VC_F / 2; cb += 16) {
+                for (int cb = 0; cb < QF; cb += 16) {
                     float vv[16];
                     tmem_ld16(taddr + (uint32_t)cb, vv);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) Ex[(lg * VC_F + half * (VC_F / 2) + cb + i) * VC_V + lane] = vv[i];
+                    for (int i = 0; i < 16; ++i) Ex[(lg * VC_F + qt * QF + cb + i) * VC_V + lane] = vv[i];
                 }
             }
             tc_fence_before();

@@ -689,6 +689,51 @@ static int solve(const real *H, const real *g, int n, real *d, float damping)
     return ok;
 }
 
+/* The shape fit's solve (Solver::solve, solver.h:70-105, for the image fit's K+6 unknowns)
+ * with reciprocal pivots: r_j = 1 / l_jj once per column, L(i,j) = t_ij * r_j; forward
+ * y_i = (g_i - sum_k L(i,k) y_k) * r_i (terms in increasing k); back x_i = (y_i -
+ * sum_k L(k,i) x_k) * r_i (terms in decreasing k); d = -x. The dot products are those of
+ * solve(); the reference's cuSOLVER order is the library's. */
+static int solve_shape(const real *H, const real *g, int n, real *d, float damping)
+{
+    double *L = (double *)malloc(sizeof(double) * n * n);
+    double *y = (double *)malloc(sizeof(double) * n);
+    double *r = (double *)malloc(sizeof(double) * n);
+    for (int i = 0; i < n * n; ++i) L[i] = (double)H[i];
+    for (int i = 0; i < n; ++i) L[i * n + i] += (double)damping;
+    int ok = 1;
+    for (int j = 0; j < n && ok; ++j) {
+        double s = L[j * n + j];
+        for (int k = 0; k < j; ++k) s -= L[k * n + j] * L[k * n + j];
+        if (!(s > 0.0)) { ok = 0; break; }
+        const double ljj = sqrt(s);
+        L[j * n + j] = ljj;
+        r[j] = 1.0 / ljj;
+        for (int i = j + 1; i < n; ++i) {
+            double t = L[j * n + i];
+            for (int k = 0; k < j; ++k) t -= L[k * n + i] * L[k * n + j];
+            L[j * n + i] = t * r[j];
+        }
+    }
+    if (ok) {
+        for (int i = 0; i < n; ++i) {
+            double t = (double)g[i];
+            for (int k = 0; k < i; ++k) t -= L[k * n + i] * y[k];
+            y[i] = t * r[i];
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double t = y[i];
+            for (int k = n - 1; k > i; --k) t -= L[i * n + k] * y[k];
+            y[i] = t * r[i];
+        }
+        for (int i = 0; i < n; ++i) d[i] = (real)(-y[i]);
+    } else {
+        for (int i = 0; i < n; ++i) d[i] = (real)NAN;
+    }
+    free(L); free(y); free(r);
+    return ok;
+}
+
 /* ------------------------------------------------------------------------------------ */
 /* Per-frame fitting context */
 
@@ -946,7 +991,7 @@ static int fit_shape(ctx_t *c, real *x, real *x_ls, const real *lam, real Lint, 
         image_normal_equations(c, tau_img, H, gv);
         double ob = barrier(m, c->f, x, c->R, c->dR, finetune, H, gv);
         grad_corr = grad_corr + (-(real)ob);
-        if (!solve(H, gv, KT, d, c->cfg->damping)) c->rep->flags |= O_FLAG_CHOL_FAILED;
+        if (!solve_shape(H, gv, KT, d, c->cfg->damping)) c->rep->flags |= O_FLAG_CHOL_FAILED;
         if (isnan((double)d[0])) { c->rep->flags |= O_FLAG_NAN_DIRECTION; terminate = 1; break; }
         real t = 1.0f;
         const real ALPHA = 0.4f, BETA = 0.8f;
@@ -1140,7 +1185,7 @@ int o_evaluate_f(const o_model *m, const o_frame *f, const o_config *cfg, const 
     const real tau_img = (real)25.0f;
     image_normal_equations(&c, tau_img, Hr, gr);
     double ob = barrier(m, f, xr, c.R, c.dR, finetune_bounds, Hr, gr);
-    if (!solve(Hr, gr, KT, dr, cfg->damping)) rep.flags |= O_FLAG_CHOL_FAILED;
+    if (!solve_shape(Hr, gr, KT, dr, cfg->damping)) rep.flags |= O_FLAG_CHOL_FAILED;
     real grad_corr = tau_img * (real)corr;
     grad_corr = grad_corr + (-(real)ob);
     if (slot) memcpy(slot, c.fr.slot, sizeof(int32_t) * N);
