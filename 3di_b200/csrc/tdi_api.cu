@@ -379,6 +379,7 @@ DBatch batch_view(const tdi_batch *bt, int f0, int nf)
     v.frag = a.frag + F0 * NMAX;
     v.fgrad = a.fgrad + F0 * 5 * NMAX;
     v.nb = a.nb + F0 * 4 * NMAX;
+    v.shc = a.shc + F0 * NMAX; v.sht = a.sht + F0 * NMAX;
     v.J = a.J + F0 * NMAX * KTP;
     v.ne_part = a.ne_part + F0 * bt->ne_frame_doubles;
     v.img = a.img + F0 * RIMG;
@@ -774,7 +775,7 @@ tdi_status tdi_batch_create(tdi_model *m, int32_t max_frames, tdi_batch **out)
     A(d.lam, F * 4); A(d.lam_ls, F * 4); A(d.lame, F * 4); A(d.dlam, F * 4); A(d.glam, F * 4);
     A(d.d, F * KTP); A(d.g, F * KTP); A(d.H, F * KTP * KTP); A(d.R, F * 9); A(d.dR, F * 27);
     A(d.ctl, F); A(d.act, F); A(d.rlist, F); A(d.rcount, F); A(d.geo, F * (size_t)md.V); A(d.proj, F * (size_t)md.V); A(d.zbuf, F * NPIX); A(d.tri_mask, F * (size_t)mask_words(md.T)); A(d.tri_list, F * (size_t)md.T); A(d.frag, F * NMAX);
-    A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX);
+    A(d.fgrad, F * 5 * NMAX); A(d.nb, F * 4 * NMAX); A(d.shc, F * NMAX); A(d.sht, F * NMAX);
     A(d.J, F * NMAX * KTP); b->ne_frame_doubles = NE_MAXCH * std::max((size_t)ne_part_stride((int)KTP), (tc_part_bytes(md.KT) + 7) / 8);
     A(d.ne_part, F * b->ne_frame_doubles); A(d.err, 1); A(d.img, F * RIMG); A(b->scalars, F * 4); A(b->d_count, 2);
     A(d.prof_frames, 1);

@@ -61,7 +61,7 @@ struct FrameCtl {
     int32_t bbox[4];     // fragment pixel box of the last raster: xmin, xmax, ymin, ymax
     float objective;     // last accepted objective
     int32_t stage_ok;    // result of the last shape fit (outer > NITERS_SUCCESS)
-    int32_t pad[1];
+    int32_t shade_cached;// the light fit's per-fragment shading terms (shc, sht) hold this raster's
 };
 
 struct Fragment {        // one surviving fragment, in slot order
@@ -133,6 +133,8 @@ struct DBatch {
     Fragment *frag;          // [F][NMAX]
     float *fgrad;            // [F][5][NMAX]: gx, gy, h, gxs_n, gys_n
     int32_t *nb;             // [F][4][NMAX]: kl, kr, ka, kb
+    float4 *shc;             // [F][NMAX]: unit normal and n . p of each fragment (light fit)
+    float *sht;              // [F][NMAX]: interpolated albedo of each fragment (light fit)
     float *J;                // [F][NMAX][KTP]
     double *ne_part;         // [F][NMAX/256][part stride] chunk partials of the normal equations
     float *img;              // [F][2][NPIX] blur scratch for frames too large for shared memory

@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=1024, help="frames per GPU per step")
-    ap.add_argument("--cpu-frames", type=int, default=8, help="frames of the CPU sample")
+    ap.add_argument("--cpu-frames", type=int, default=24, help="frames of the CPU sample (about 10 s of CPU work)")
     ap.add_argument("--plain-frames", type=int, default=16, help="frames of the unbatched (plain) run")
     ap.add_argument("--normal-eq", default="exact", choices=["exact", "tensor"],
                     help="normal equations: FP64 in the oracle's order, or split-BF16 on the tensor cores")
