@@ -86,6 +86,7 @@ SIGNATURES = {
     "tdi_batch_set_video_frames": (C.c_int32, [C.c_void_p, C.POINTER(VideoFramesDesc), C.c_void_p]),
     "tdi_orthographic_init": (C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tdi_apply_identity": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32] + [C.c_void_p] * 9),
     "tdi_batch_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_landmark_init": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdi_batch_loss": (C.c_int32, [C.c_void_p, C.POINTER(FitConfig), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -207,6 +208,25 @@ class Model:
             self.close()
         except Exception:
             pass
+
+
+def apply_identity(mean0, id_basis, alpha, tex0, tex_basis, beta):
+    """The subject's shape and albedo (tdi_apply_identity): mean0 [3][V] + id_basis [3][V][Ka] .
+    alpha, tex0 [V] + tex_basis [V][Kb] . beta, on the device. Returns (mean [3][V], tex [V])."""
+    mean0, tex0 = _f32(mean0), _f32(tex0)
+    V = mean0.shape[1]
+    KA = 0 if id_basis is None else int(np.shape(id_basis)[2])
+    KB = 0 if tex_basis is None else int(np.shape(tex_basis)[1])
+    I = _f32(id_basis) if KA else None
+    a = _f32(alpha) if KA else None
+    T = _f32(tex_basis) if KB else None
+    bt = _f32(beta) if KB else None
+    mean = np.zeros((3, V), np.float32)
+    tex = np.zeros(V, np.float32)
+    ptr = lambda x: _p(x) if x is not None else None
+    _check(load_library().tdi_apply_identity(V, KA, KB, _p(mean0), ptr(I), ptr(a), _p(tex0), ptr(T), ptr(bt),
+                                             _p(mean), _p(tex), None))
+    return mean, tex
 
 
 def orthographic_init(xl, yl, p0L):

@@ -1084,6 +1084,44 @@ static void euler_degrees(const float *R, float *ypr)
     ypr[2] = (float)((double)(roll * 180.0f) / M_PI);
 }
 
+tdi_status tdi_apply_identity(int32_t n_vertices, int32_t n_id, int32_t n_tex, const float *mean0,
+                              const float *id_basis, const float *alpha, const float *tex0,
+                              const float *tex_basis, const float *beta, float *mean, float *tex,
+                              void *stream)
+{
+    if (n_vertices <= 0 || n_id < 0 || n_tex < 0 || !mean0 || !tex0 || !mean || !tex ||
+        (n_id > 0 && (!id_basis || !alpha)) || (n_tex > 0 && (!tex_basis || !beta)))
+        return fail(TDI_ERR_INVALID, "bad identity arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t V = (size_t)n_vertices, KA = (size_t)n_id, KB = (size_t)n_tex;
+    const size_t nf = 4 * V + 3 * V * KA + KA + V * KB + KB;
+    float *buf = nullptr;
+    TDI_CUDA(cudaMalloc(&buf, nf * sizeof(float)));
+    float *dm = buf, *dt = dm + 3 * V, *dI = dt + V, *da = dI + 3 * V * KA, *dT = da + KA, *db = dT + V * KB;
+    auto run = [&]() -> tdi_status {
+        TDI_CUDA(cudaMemcpyAsync(dm, mean0, 3 * V * sizeof(float), cudaMemcpyHostToDevice, s));
+        TDI_CUDA(cudaMemcpyAsync(dt, tex0, V * sizeof(float), cudaMemcpyHostToDevice, s));
+        if (KA) {
+            TDI_CUDA(cudaMemcpyAsync(dI, id_basis, 3 * V * KA * sizeof(float), cudaMemcpyHostToDevice, s));
+            TDI_CUDA(cudaMemcpyAsync(da, alpha, KA * sizeof(float), cudaMemcpyHostToDevice, s));
+        }
+        if (KB) {
+            TDI_CUDA(cudaMemcpyAsync(dT, tex_basis, V * KB * sizeof(float), cudaMemcpyHostToDevice, s));
+            TDI_CUDA(cudaMemcpyAsync(db, beta, KB * sizeof(float), cudaMemcpyHostToDevice, s));
+        }
+        const unsigned blocks = (unsigned)((4 * V + 255) / 256);
+        k_apply_identity<<<blocks, 256, 0, s>>>((int)V, (int)KA, (int)KB, dm, dI, da, dt, dT, db);
+        TDI_CUDA(cudaGetLastError());
+        TDI_CUDA(cudaMemcpyAsync(mean, dm, 3 * V * sizeof(float), cudaMemcpyDeviceToHost, s));
+        TDI_CUDA(cudaMemcpyAsync(tex, dt, V * sizeof(float), cudaMemcpyDeviceToHost, s));
+        TDI_CUDA(cudaStreamSynchronize(s));
+        return TDI_OK;
+    };
+    const tdi_status st = run();
+    cudaFree(buf);
+    return st;
+}
+
 tdi_status tdi_orthographic_init(int32_t n_frames, const float *xl, const float *yl, const float *p0L,
                                  float *x_out, float *ypr_out, int32_t *iters_out, void *stream)
 {

@@ -2195,6 +2195,8 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
             ci[a] = (i > j && i < n) ? rj[i] * r : 0.0;
             cl[a] = (l > j && l < n) ? rj[l] * r : 0.0;
         }
+        // (skipping finished 16-row or 16-column blocks by block-uniform tests measured slower:
+        // 1.36 against 1.19 us per frame-evaluation)
 #pragma unroll
         for (int a = 0; a < RB; ++a)
 #pragma unroll
@@ -2520,6 +2522,30 @@ __global__ void __launch_bounds__(1024) k_compact_active(DBatch b, int *out)
     if (tid == 0) {
         out[0] = s_base;
         out[1] = *b.err;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// The subject's shape and albedo (renderer.cu:866-883,941-951): one thread per coordinate of a
+// vertex (rows 0..3V-1: X, Y, Z planes) or albedo entry (rows 3V..4V-1); the basis row is a
+// sequential fused multiply-add chain over k from 0, then added to the mean. In place on m, t.
+
+__global__ void k_apply_identity(int V, int KA, int KB, float *m, const float *I, const float *alpha, float *t,
+                                 const float *T, const float *beta)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= 4 * V) return;
+    if (r < 3 * V) {
+        const float *row = I + (size_t)r * KA;
+        float acc = 0.0f;
+        for (int k = 0; k < KA; ++k) acc = fmaf(row[k], alpha[k], acc);
+        if (KA) m[r] = m[r] + acc;
+    } else {
+        const int v = r - 3 * V;
+        const float *row = T + (size_t)v * KB;
+        float acc = 0.0f;
+        for (int k = 0; k < KB; ++k) acc = fmaf(row[k], beta[k], acc);
+        if (KB) t[v] = t[v] + acc;
     }
 }
 

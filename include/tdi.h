@@ -101,6 +101,19 @@ typedef struct {
  * xl, yl [F][51], from the reference's start point. Outputs x [F][7], the yaw, pitch and roll
  * in degrees of the last trial rotation [F][3] (or NULL) and the outer iterations [F]
  * (or NULL). Host arrays; allocates its device buffers; synchronous. */
+/* The subject's shape and albedo from identity and texture coefficients: the reference's
+ * Renderer::compute_nonrigid_shape_identityonly and compute_texture (renderer.cu:866-883,941-951;
+ * cublasSgemv there): mean[c][v] = mean0[c][v] + sum_k id_basis[c][v][k] alpha[k] (c = X, Y, Z)
+ * and tex[v] = tex0[v] + sum_k tex_basis[v][k] beta[k], each sum a sequential FP32 fused
+ * multiply-add chain over k from 0, added to the mean last (the reference's summation order is
+ * the library's). Host arrays: mean0 [3][V], id_basis [3][V][n_id] (IX/IY/IZ.dat rows), alpha
+ * [n_id], tex0 [V], tex_basis [V][n_tex] (TEX.dat rows), beta [n_tex]; outputs mean [3][V] and
+ * tex [V], the inputs of tdi_model_create. n_id or n_tex may be 0 (a copy). Synchronous. */
+tdi_status tdi_apply_identity(int32_t n_vertices, int32_t n_id, int32_t n_tex, const float *mean0,
+                              const float *id_basis, const float *alpha, const float *tex0,
+                              const float *tex_basis, const float *beta, float *mean, float *tex,
+                              void *stream);
+
 tdi_status tdi_orthographic_init(int32_t n_frames, const float *xl, const float *yl, const float *p0L,
                                  float *x_out, float *ypr_out, int32_t *iters_out, void *stream);
 

@@ -267,5 +267,22 @@ def landmark_init(model: Model, frames: FrameSet, j: int, p0L, kind="f32"):
     return x, slack.value, bool(ok), newton.value, bool(flip.value)
 
 
+def apply_identity(mean0, id_basis, alpha, tex0, tex_basis, beta):
+    """The subject's shape and albedo: mean0 + id_basis . alpha, tex0 + tex_basis . beta
+    (o_apply_identity; FP32 fused multiply-add chains)."""
+    mean0, tex0 = _f32(mean0), _f32(tex0)
+    V = mean0.shape[1]
+    KA = 0 if id_basis is None else int(np.shape(id_basis)[2])
+    KB = 0 if tex_basis is None else int(np.shape(tex_basis)[1])
+    I = _f32(id_basis) if KA else np.zeros(1, np.float32)
+    a = _f32(alpha) if KA else np.zeros(1, np.float32)
+    T = _f32(tex_basis) if KB else np.zeros(1, np.float32)
+    b = _f32(beta) if KB else np.zeros(1, np.float32)
+    mean = np.zeros((3, V), np.float32)
+    tex = np.zeros(V, np.float32)
+    lib("f32").o_apply_identity(V, KA, KB, _p(mean0), _p(I), _p(a), _p(tex0), _p(T), _p(b), _p(mean), _p(tex))
+    return mean, tex
+
+
 def max_threads(kind="f32") -> int:
     return int(lib(kind).o_max_threads())

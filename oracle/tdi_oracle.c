@@ -1685,3 +1685,24 @@ int o_landmark_init_f(const o_model *m, const o_frame *f, const float *p0L, floa
     free(o.F); free(o.nWx); free(o.nWy); free(H); free(g); free(d); free(z); free(zt);
     return success;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* Renderer::compute_nonrigid_shape_identityonly and compute_texture (renderer.cu:866-883,
+ * 941-951): mean[c][v] = mean0[c][v] + (sequential fmaf chain over k of id[c][v][k] alpha[k])
+ * and tex[v] = tex0[v] + (the same over TEX[v][k] beta[k]); n_id or n_tex 0 leaves a copy. The
+ * reference's cublasSgemv order is the library's; this order is the contract shared with the
+ * device. FP32 in both builds. */
+void o_apply_identity(int V, int KA, int KB, const float *mean0, const float *I, const float *alpha,
+                      const float *tex0, const float *T, const float *beta, float *mean, float *tex)
+{
+    for (int r = 0; r < 3 * V; ++r) {
+        float acc = 0.0f;
+        for (int k = 0; k < KA; ++k) acc = fmaf(I[(size_t)r * KA + k], alpha[k], acc);
+        mean[r] = KA ? mean0[r] + acc : mean0[r];
+    }
+    for (int v = 0; v < V; ++v) {
+        float acc = 0.0f;
+        for (int k = 0; k < KB; ++k) acc = fmaf(T[(size_t)v * KB + k], beta[k], acc);
+        tex[v] = KB ? tex0[v] + acc : tex0[v];
+    }
+}
