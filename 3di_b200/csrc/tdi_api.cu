@@ -178,9 +178,11 @@ struct tdi_batch {
     int64_t launches = 0;          // kernels launched by this batch
     int prof_id = 0;               // kernel timed by tdi_batch_profile
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
-    // CUDA graphs of GRAPH_ROUNDS rounds of a stage, per (stage, capacity tier, frames, config)
+    // CUDA graphs of GRAPH_ROUNDS rounds of a stage, per (lane, stage, capacity tier, frames,
+    // config)
     struct RoundGraph {
-        int stage, tier, F;
+        int lane, stage, tier, F;
+        const FrameCtl *ctl;       // the lane's first frame (its view of the batch)
         Cfg cfg;
         cudaGraphExec_t exec;
         int64_t kernels;           // kernel nodes in the graph
@@ -190,10 +192,14 @@ struct tdi_batch {
 
 namespace {
 
-// Streams a batched fit runs on. Two lanes (halves of the batch on two streams) measured
-// slower than one on B200 once the per-frame kernels filled the SMs by themselves: 3,235
-// against 3,437 frames/s on the 1,024-frame video fit, so the batch runs as one lane.
-constexpr int FIT_LANES = 1;
+// Streams a batched fit runs on: lanes are parts of the batch with their own stream, active
+// list and round graphs, replayed side by side so that one lane's latency-bound rounds (few
+// frames still running, one block per frame) overlap the other's work.
+#ifndef TDI_FIT_LANES
+#define TDI_FIT_LANES 1
+#endif
+constexpr int FIT_LANES = TDI_FIT_LANES;
+static_assert(FIT_LANES >= 1 && FIT_LANES <= 8, "lanes of a fit");
 constexpr int FIT_LANE_MIN = 32;   // frames a lane needs before a batch is split
 
 template <typename T>
@@ -273,7 +279,8 @@ tdi_status set_attrs()
                                   RENDER_SMEM_FLOATS * (int)sizeof(float)));
     TDI_CUDA(cudaFuncSetAttribute(k_neighbours, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)neigh_smem()));
-    TDI_CUDA(cudaFuncSetAttribute(k_vertex, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_vertex_t<VT_FPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_vertex_t<VT_FPT_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_barrier_full, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -285,8 +292,9 @@ tdi_status set_attrs()
     return TDI_OK;
 }
 
-// Vertex stage grid: frame tiles x vertex-tile groups, about VT_BLOCKS_PER_SM blocks per SM.
-dim3 vertex_grid(const DModel &m, int frames)
+// Vertex stage grid: frame tiles of nf frames x vertex-tile groups, about VT_BLOCKS_PER_SM
+// blocks per SM.
+dim3 vertex_grid(const DModel &m, int frames, int nf = VT_F)
 {
     static int sms = 0;
     if (!sms) {
@@ -296,9 +304,24 @@ dim3 vertex_grid(const DModel &m, int frames)
     }
     // the kernel splits the blocks between frame tiles and vertex stripes by the number of
     // frames that render, which is at most `frames`
-    const long ftiles = std::max(1, (frames + VT_F - 1) / VT_F);
+    const long ftiles = std::max(1, (frames + nf - 1) / nf);
     const long ntiles = (m.V + VT_V - 1) / VT_V;
     return dim3((unsigned)std::max(ftiles, std::min((long)VT_BLOCKS_PER_SM * sms, ftiles * ntiles)));
+}
+
+// The exact vertex stage for at most `frames` rendering frames: 8 frames per thread (64-frame
+// tiles) for full rounds; 2 per thread (16-frame tiles) when at most VT_SMALL frames can render,
+// where a 64-frame tile would carry mostly idle frames through every multiply-add.
+constexpr int VT_SMALL = 32;
+
+template <class B>
+tdi_status launch_vertex(B *bt, const DModel &m, const DBatch &d, cudaStream_t s, int frames)
+{
+    if (frames <= VT_SMALL)
+        return launch(bt, KID_VERTEX, k_vertex_t<VT_FPT_SMALL>, vertex_grid(m, frames, 8 * VT_FPT_SMALL),
+                      dim3(32, VT_WARPS + 1), vt_smem(m.KP, 8 * VT_FPT_SMALL), s, m, d);
+    return launch(bt, KID_VERTEX, k_vertex_t<VT_FPT>, vertex_grid(m, frames), dim3(32, VT_WARPS + 1),
+                  vt_smem(m.KP), s, m, d);
 }
 
 // Tensor-core vertex stage: one block per SM, split between frame tiles and vertex stripes.
@@ -335,7 +358,6 @@ struct Launch {
     const DBatch &b;
     cudaStream_t s;
     int F;
-    size_t smem_vertex() const { return vt_smem(m.KP); }
     size_t smem_neigh() const { return neigh_smem(); }
     size_t smem_ne() const { return (size_t)2 * 2 * NE_SUB * NE_PD * sizeof(double); }
     size_t smem_bar() const { return (size_t)4 * NL * NE_P8 * sizeof(float); }
@@ -427,7 +449,7 @@ tdi_status geometry(const Launch &L, const Cfg &c, int stage)
         TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex_tc, vertex_tc_grid(L.m, L.A()), dim3(VC_THREADS), vc_smem(L.m.K),
                        L.s, L.m, L.b, reinterpret_cast<const __nv_bfloat16 *>(L.m.Etc)));
     else
-        TDI_TRY(launch(L.bt, KID_VERTEX, k_vertex, vertex_grid(L.m, L.A()), dim3(32, VT_WARPS + 1), L.smem_vertex(), L.s, L.m, L.b));
+        TDI_TRY(launch_vertex(L.bt, L.m, L.b, L.s, L.A()));
     TDI_TRY(launch(L.bt, KID_RASTER, k_raster_depth, dim3(raster_blocks(L.A()), L.A()), dim3(RD_THREADS), 0, L.s, L.m, L.b));
     TDI_TRY(launch(L.bt, KID_RESOLVE, k_raster_resolve, dim3(L.A()), dim3(RR_THREADS), 0, L.s, L.m, L.b));
     return TDI_OK;
@@ -501,10 +523,12 @@ int graph_tier(int n, int F)
     return F;
 }
 
-tdi_status stage_graph(tdi_batch *bt, const Cfg &c, int stage, tdi_lane &ln, int tier, tdi_batch::RoundGraph **out)
+tdi_status stage_graph(tdi_batch *bt, const Cfg &c, int stage, int lane, int tier, tdi_batch::RoundGraph **out)
 {
+    tdi_lane &ln = bt->lanes[lane];
     for (auto &g : bt->graphs)
-        if (g.stage == stage && g.tier == tier && g.F == ln.d.F && std::memcmp(&g.cfg, &c, sizeof(Cfg)) == 0) {
+        if (g.lane == lane && g.stage == stage && g.tier == tier && g.F == ln.d.F && g.ctl == ln.d.ctl &&
+            std::memcmp(&g.cfg, &c, sizeof(Cfg)) == 0) {
             *out = &g;
             return TDI_OK;
         }
@@ -529,36 +553,52 @@ tdi_status stage_graph(tdi_batch *bt, const Cfg &c, int stage, tdi_lane &ln, int
     const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) return fail(TDI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
-    bt->graphs.push_back({stage, tier, ln.d.F, c, exec, kernels});
+    bt->graphs.push_back({lane, stage, tier, ln.d.F, ln.d.ctl, c, exec, kernels});
     *out = &bt->graphs.back();
     return TDI_OK;
 }
 
-// A stage with its rounds replayed from graphs (one lane, no live profiling).
-tdi_status run_stage_graphs(tdi_batch *bt, const Cfg &c, int stage)
+// A stage with its rounds replayed from graphs (no live profiling): every lane's replay is
+// enqueued on its stream before any lane's count is read back.
+tdi_status run_stage_graphs(tdi_batch *bt, const Cfg &c, int stage, int nlanes)
 {
     const DModel &m = bt->m->d;
-    tdi_lane &ln = bt->lanes[0];
-    TDI_TRY(launch(bt, 0, k_stage_start, dim3((ln.d.F + 127) / 128), dim3(128), 0, ln.s, m, ln.d, c, stage));
-    TDI_TRY(lane_compact(bt, ln));
-    TDI_TRY(lane_count(ln));
+    for (int l = 0; l < nlanes; ++l) {
+        tdi_lane &ln = bt->lanes[l];
+        TDI_TRY(launch(bt, 0, k_stage_start, dim3((ln.d.F + 127) / 128), dim3(128), 0, ln.s, m, ln.d, c, stage));
+        TDI_TRY(lane_compact(bt, ln));
+    }
+    for (int l = 0; l < nlanes; ++l) TDI_TRY(lane_count(bt->lanes[l]));
     const long max_rounds = stage == ST_LAMBDA ? 8L * c.max_iters_lambda + 16
                                                : 16L * (stage == ST_RIGID ? c.max_iters_rigid : c.max_iters_finetune) + 16;
-    long round = 0;
-    if (stage == ST_LAMBDA && ln.n > 0) {       // the light fit's first round also rasterises
-        TDI_TRY(stage_round(bt, c, stage, ln.d, ln.s, 0));
-        TDI_TRY(lane_compact(bt, ln));
-        TDI_TRY(lane_count(ln));
-        round = 1;
+    long round[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (stage == ST_LAMBDA) {                   // the light fit's first round also rasterises
+        for (int l = 0; l < nlanes; ++l) {
+            tdi_lane &ln = bt->lanes[l];
+            if (ln.n <= 0) continue;
+            TDI_TRY(stage_round(bt, c, stage, ln.d, ln.s, 0));
+            TDI_TRY(lane_compact(bt, ln));
+            round[l] = 1;
+        }
+        for (int l = 0; l < nlanes; ++l)
+            if (round[l]) TDI_TRY(lane_count(bt->lanes[l]));
     }
-    while (ln.n > 0 && round < max_rounds) {
-        tdi_batch::RoundGraph *g = nullptr;
-        TDI_TRY(stage_graph(bt, c, stage, ln, graph_tier(ln.n, ln.d.F), &g));
-        TDI_CUDA(cudaGraphLaunch(g->exec, ln.s));
-        bt->launches += g->kernels;
-        TDI_CUDA(cudaMemcpyAsync(ln.h_count, ln.d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, ln.s));
-        TDI_TRY(lane_count(ln));
-        round += GRAPH_ROUNDS;
+    for (;;) {
+        bool launched[8] = {false, false, false, false, false, false, false, false}, any = false;
+        for (int l = 0; l < nlanes; ++l) {
+            tdi_lane &ln = bt->lanes[l];
+            if (ln.n <= 0 || round[l] >= max_rounds) continue;
+            tdi_batch::RoundGraph *g = nullptr;
+            TDI_TRY(stage_graph(bt, c, stage, l, graph_tier(ln.n, ln.d.F), &g));
+            TDI_CUDA(cudaGraphLaunch(g->exec, ln.s));
+            bt->launches += g->kernels;
+            TDI_CUDA(cudaMemcpyAsync(ln.h_count, ln.d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, ln.s));
+            round[l] += GRAPH_ROUNDS;
+            launched[l] = any = true;
+        }
+        if (!any) break;
+        for (int l = 0; l < nlanes; ++l)
+            if (launched[l]) TDI_TRY(lane_count(bt->lanes[l]));
     }
     return TDI_OK;
 }
@@ -567,7 +607,7 @@ tdi_status run_stage_graphs(tdi_batch *bt, const Cfg &c, int stage)
 // the lanes' rounds are enqueued on their own streams before any lane is waited for.
 tdi_status run_stage_lanes(tdi_batch *bt, const Cfg &c, int stage, int nlanes)
 {
-    if (nlanes == 1 && !c.host_rounds && bt->prof_id == 0) return run_stage_graphs(bt, c, stage);
+    if (!c.host_rounds && bt->prof_id == 0) return run_stage_graphs(bt, c, stage, nlanes);
     const DModel &m = bt->m->d;
     for (int l = 0; l < nlanes; ++l) {
         tdi_lane &ln = bt->lanes[l];
@@ -1250,7 +1290,7 @@ static tdi_status adj_forward(tdi_batch *b, const Cfg &c, const float *x, const 
     if (n > 0) {
         TDI_TRY(launch(b, 0, k_prepare, Lc.wblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
         TDI_TRY(launch(b, 0, k_compact_render, dim3(1), dim3(1024), 0, s, (const DBatch)d));
-        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, VT_WARPS + 1), Lc.smem_vertex(), s, m, d));
+        TDI_TRY(launch_vertex(b, m, d, s, n));
         TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(raster_blocks(n), n), dim3(RD_THREADS), 0, s, m, d));
         TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));
     }
@@ -1456,7 +1496,7 @@ tdi_status tdi_batch_render(tdi_batch *b, float *images, int32_t *tri_map, void 
     if (n > 0) {
         TDI_TRY(launch(b, 0, k_prepare, L.wblocks(), dim3(128), 0, s, m, d, (int)ST_RIGID));
         TDI_TRY(launch(b, 0, k_compact_render, dim3(1), dim3(1024), 0, s, (const DBatch)d));
-        TDI_TRY(launch(b, KID_VERTEX, k_vertex, vertex_grid(m, n), dim3(32, VT_WARPS + 1), L.smem_vertex(), s, m, d));
+        TDI_TRY(launch_vertex(b, m, d, s, n));
         TDI_TRY(launch(b, KID_RASTER, k_raster_depth, dim3(raster_blocks(n), n), dim3(RD_THREADS), 0, s, m, d));
         TDI_TRY(launch(b, KID_RESOLVE, k_raster_resolve, dim3(n), dim3(RR_THREADS), 0, s, m, d));
     }

@@ -208,20 +208,40 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c)
 }
 
 constexpr int VT_V = 32;                                   // vertices per tile (one per lane)
-constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block
+constexpr int VT_FPT = 8, VT_F = 8 * VT_FPT;               // frames per thread, per block (full rounds)
+constexpr int VT_FPT_SMALL = 2;                             // frames per thread when few frames render
 constexpr int VT_FR = 16;                                   // per-frame floats: R(9), tau(3), cam(4)
 constexpr int VT_BLOCKS_PER_SM = 2;
 constexpr int VT_WARPS = 8;                                 // computing warps; one more issues the copies
 constexpr int VT_THREADS = (VT_WARPS + 1) * 32;
 
 __host__ __device__ __forceinline__ int vt_row(int KP) { return 3 * KP + 4; }   // basis row pitch (floats)
-__host__ __device__ __forceinline__ size_t vt_smem(int KP)
+__host__ __device__ __forceinline__ size_t vt_smem(int KP, int NF = VT_F)
 {
-    return ((size_t)2 * VT_V * vt_row(KP) + (size_t)VT_F * KP + (size_t)VT_F * VT_FR) * sizeof(float);
+    return ((size_t)2 * VT_V * vt_row(KP) + (size_t)NF * KP + (size_t)NF * VT_FR) * sizeof(float);
 }
 
-__global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel m, DBatch b)
+// A thread's FPT coefficients at one k as frame pairs (16-byte loads for 8, 8-byte for 2).
+template <int FPT>
+__device__ __forceinline__ void vt_load_x(float2 (&xv)[FPT / 2], const float *p)
 {
+    if constexpr (FPT == 8) {
+        const float4 xa = *reinterpret_cast<const float4 *>(p), xb = *reinterpret_cast<const float4 *>(p + 4);
+        xv[0] = make_float2(xa.x, xa.y); xv[1] = make_float2(xa.z, xa.w);
+        xv[2] = make_float2(xb.x, xb.y); xv[3] = make_float2(xb.z, xb.w);
+    } else {
+#pragma unroll
+        for (int q = 0; q < FPT / 2; ++q) xv[q] = *reinterpret_cast<const float2 *>(p + 2 * q);
+    }
+}
+
+// FPT frames per computing thread, 8 FPT per block: 8 for full rounds; 2 when few frames render
+// (a 64-frame tile then carries mostly idle frames through every multiply-add).
+template <int FPT>
+__global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex_t(DModel m, DBatch b)
+{
+    constexpr int VT_F = 8 * FPT;              // frames of a block tile
+    constexpr int VT_FPT = FPT;
     extern __shared__ __align__(16) float vsm[];
     const int KP = m.KP, K = m.K, ER = vt_row(KP);
     float *Eb = vsm;                           // [2][VT_V][ER]: basis rows of two tiles
@@ -316,7 +336,7 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
         }
     } else {
         const int vl = threadIdx.x;
-        const float *xr = Xs + threadIdx.y * VT_FPT;      // this warp's 8 frames at k: xr[k * VT_F + q]
+        const float *xr = Xs + threadIdx.y * VT_FPT;      // this warp's frames at k: xr[k * VT_F + q]
         for (int j = 0;; ++j) {
             const int t = gy + j * groups;
             if (t >= ntiles) break;
@@ -346,10 +366,8 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
                 const float ezv[4] = {ez.x, ez.y, ez.z, ez.w};
 #pragma unroll
                 for (int jj = 0; jj < 4; ++jj) {
-                    const float4 xa = *reinterpret_cast<const float4 *>(xr + (k + jj) * VT_F);
-                    const float4 xb = *reinterpret_cast<const float4 *>(xr + (k + jj) * VT_F + 4);
-                    const float2 xv[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
-                                          make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
+                    float2 xv[VT_FPT / 2];
+                    vt_load_x<VT_FPT>(xv, xr + (k + jj) * VT_F);
                     const float2 e0 = make_float2(exv[jj], exv[jj]), e1 = make_float2(eyv[jj], eyv[jj]);
                     const float2 e2 = make_float2(ezv[jj], ezv[jj]);
 #pragma unroll
@@ -362,10 +380,8 @@ __global__ void __launch_bounds__(VT_THREADS, VT_BLOCKS_PER_SM) k_vertex(DModel 
             }
             for (; k < K; ++k) {
                 const float ex = er[k], ey = er[KP + k], ez = er[2 * KP + k];
-                const float4 xa = *reinterpret_cast<const float4 *>(xr + k * VT_F);
-                const float4 xb = *reinterpret_cast<const float4 *>(xr + k * VT_F + 4);
-                const float2 xv[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
-                                      make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
+                float2 xv[VT_FPT / 2];
+                vt_load_x<VT_FPT>(xv, xr + k * VT_F);
 #pragma unroll
                 for (int q = 0; q < VT_FPT / 2; ++q) {
                     acc[q][0] = ffma2(make_float2(ex, ex), xv[q], acc[q][0]);
