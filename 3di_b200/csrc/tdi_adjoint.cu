@@ -88,6 +88,70 @@ __global__ void k_adj_rot(DModel m, DBatch b, const float *x, int F, double *R64
 
 // FP64 vertex stage: object coordinates P0 = mean + E eps, camera X = R P0 + tau, projections.
 // geo64 [F][V][8]: P0 (3), X (3), xp, yp.
+// The same per (frame, vertex), tiled: a block takes AV_V vertices x AV_F frames, stages their
+// basis rows and coefficients in shared memory once (instead of every thread reading its
+// vertex's rows from L2 for every frame), and each thread forms one vertex of AV_F / 8 frames;
+// the fused multiply-add chains over k are the same, in the same order.
+constexpr int AV_V = 32, AV_F = 32, AV_FPT = AV_F / 8;
+
+__host__ __device__ __forceinline__ size_t adj_vertex_smem(int KP)
+{
+    return ((size_t)AV_V * 3 + AV_F) * (size_t)(KP + 1) * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256) k_adj_vertex_tiled(DModel m, const float *x, int F, const double *R64,
+                                                          const float *cam, double *geo64)
+{
+    extern __shared__ float avs[];
+    const int KP = m.KP, K = m.K, KT = m.KT, W = KP + 1;    // row pitch KP + 1: lanes (vertices) on distinct banks
+    float *Es = avs;                                          // [AV_V][3][W]
+    float *Xs = Es + (size_t)AV_V * 3 * W;                   // [AV_F][W]
+    const int v0 = blockIdx.x * AV_V, f0 = blockIdx.y * AV_F, tid = threadIdx.x;
+    for (int i = tid; i < AV_V * 3 * KP; i += 256) {
+        const int r = i / KP, k = i - r * KP, v = v0 + r / 3;
+        Es[(size_t)r * W + k] = v < m.V ? m.E[(size_t)v0 * 3 * KP + i] : 0.0f;
+    }
+    for (int i = tid; i < AV_F * KP; i += 256) {
+        const int fl = i / KP, k = i - fl * KP, f = f0 + fl;
+        Xs[(size_t)fl * W + k] = (f < F && k < K) ? x[(size_t)f * KT + k] : 0.0f;
+    }
+    __syncthreads();
+    const int vl = tid & 31, fg = tid >> 5, v = v0 + vl;
+    const float *e0 = Es + (size_t)vl * 3 * W, *e1 = e0 + W, *e2 = e1 + W;
+    double acc[AV_FPT][3];
+#pragma unroll
+    for (int q = 0; q < AV_FPT; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
+    for (int k = 0; k < K; ++k) {
+        const double a0 = e0[k], a1 = e1[k], a2 = e2[k];
+#pragma unroll
+        for (int q = 0; q < AV_FPT; ++q) {
+            const double xv = Xs[(size_t)(fg * AV_FPT + q) * W + k];
+            acc[q][0] = fma(a0, xv, acc[q][0]);
+            acc[q][1] = fma(a1, xv, acc[q][1]);
+            acc[q][2] = fma(a2, xv, acc[q][2]);
+        }
+    }
+    if (v >= m.V) return;
+    const double mean[3] = {(double)m.mean[v], (double)m.mean[(size_t)m.V + v], (double)m.mean[2 * (size_t)m.V + v]};
+#pragma unroll
+    for (int q = 0; q < AV_FPT; ++q) {
+        const int f = f0 + fg * AV_FPT + q;
+        if (f >= F) break;
+        const float *xf = x + (size_t)f * KT;
+        double P[3];
+        for (int c = 0; c < 3; ++c) P[c] = mean[c] + acc[q][c];
+        const double *R = R64 + (size_t)f * 36;
+        double X[3];
+        for (int i = 0; i < 3; ++i) X[i] = (R[i] * P[0] + R[3 + i] * P[1]) + R[6 + i] * P[2] + (double)xf[K + i];
+        const float *cm = cam + (size_t)f * 4;
+        double *g = geo64 + ((size_t)f * m.V + v) * 8;
+        g[0] = P[0]; g[1] = P[1]; g[2] = P[2];
+        g[3] = X[0]; g[4] = X[1]; g[5] = X[2];
+        g[6] = (double)cm[0] * X[0] / X[2] + (double)cm[2];
+        g[7] = (double)cm[1] * X[1] / X[2] + (double)cm[3];
+    }
+}
+
 __global__ void k_adj_vertex(DModel m, const float *x, int F, const double *R64, const float *cam, double *geo64)
 {
     const int f = blockIdx.y;
@@ -366,25 +430,55 @@ __global__ void k_adj_vertex_back(DModel m, int F, const double *geo64, const do
         }
     }
     // the per-fragment rotation terms are indexed by q_k = sum_j R[3k + j] (lam - tau)_j: both
-    // index the same storage, so they add up entry by entry
+    // index the same storage, so they add up entry by entry; summed per warp, then per block,
+    // one atomic per block and entry
+    __shared__ double s_acc[8][12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) warp_atomic_add(glob + (size_t)f * AD_GLOB + i, acc[i]);
+    for (int i = 0; i < 12; ++i) {
+        const double w = wsum(acc[i]);
+        if ((threadIdx.x & 31) == 0) s_acc[threadIdx.x >> 5][i] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_acc[w][threadIdx.x];
+        atomicAdd(glob + (size_t)f * AD_GLOB + threadIdx.x, t);
+    }
 }
 
 // Basis-transpose product dL/deps_k = sum_v sum_c E[v][c][k] dL/dP0[v][c] over a tile of vertices.
 constexpr int AD_VT = 256;
+// A block takes AD_VT vertices x AE_F frames (threads = expression columns), so that each
+// basis row is read once per AE_F frames; per frame and column the vertex terms are summed in
+// vertex order, the block's partial added with one atomic.
+constexpr int AE_F = 16;
+
 __global__ void k_adj_eps(DModel m, int F, const double *dP0, double *geps)
 {
-    const int f = blockIdx.y, k = threadIdx.x;
-    if (f >= F || k >= m.K) return;
+    const int k = threadIdx.x, f0 = blockIdx.y * AE_F;
     const int v0 = blockIdx.x * AD_VT, v1 = min(m.V, v0 + AD_VT);
-    double acc = 0.0;
+    const bool live = k < m.K;
+    double acc[AE_F];
+#pragma unroll
+    for (int q = 0; q < AE_F; ++q) acc[q] = 0.0;
     for (int v = v0; v < v1; ++v) {
-        const double *P = dP0 + ((size_t)f * m.V + v) * 3;
-        const float *e = m.E + (size_t)v * 3 * m.KP + k;
-        acc += (double)e[0] * P[0] + (double)e[m.KP] * P[1] + (double)e[2 * m.KP] * P[2];
+        const float *e = m.E + (size_t)v * 3 * m.KP + (live ? k : 0);
+        const double e0 = e[0], e1 = e[m.KP], e2 = e[2 * m.KP];
+#pragma unroll
+        for (int q = 0; q < AE_F; ++q) {
+            const int f = f0 + q;
+            if (f >= F) break;
+            const double *P = dP0 + ((size_t)f * m.V + v) * 3;
+            acc[q] += e0 * P[0] + e1 * P[1] + e2 * P[2];
+        }
     }
-    atomicAdd(geps + (size_t)f * m.K + k, acc);
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < AE_F; ++q) {
+        const int f = f0 + q;
+        if (f >= F) break;
+        atomicAdd(geps + (size_t)f * m.K + k, acc[q]);
+    }
 }
 
 // Gradients out: x [F][K+6] (epsilon, tau, u through dR/du), lambda [F][3], L [F].

@@ -271,6 +271,8 @@ float face_size_of(const float *xl, const float *yl)
 }
 
 
+constexpr int ADJ_VERTEX_SMEM_MAX = 100 * 1024;   // the tiled FP64 vertex stage of the loss (K up to ~190)
+
 tdi_status set_attrs()
 {
     static bool done = false;
@@ -288,6 +290,7 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<NE_GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<TC_MAXN / 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     TDI_CUDA(cudaFuncSetAttribute(k_vertex_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vc_smem(VC_MAXK)));
+    TDI_CUDA(cudaFuncSetAttribute(k_adj_vertex_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, ADJ_VERTEX_SMEM_MAX));
     done = true;
     return TDI_OK;
 }
@@ -1297,8 +1300,12 @@ static tdi_status adj_forward(tdi_batch *b, const Cfg &c, const float *x, const 
     const size_t np = (size_t)F * NPIX;
     const dim3 pb((unsigned)((np + 255) / 256));
     TDI_TRY(launch(b, 0, k_adj_rot, dim3((F + 127) / 128), dim3(128), 0, s, m, d, x, F, o.R));
-    TDI_TRY(launch(b, 0, k_adj_vertex, dim3((m.V + 255) / 256, F), dim3(256), 0, s, m, x, F, (const double *)o.R,
-                   (const float *)d.cam, o.geo));
+    if (adj_vertex_smem(m.KP) <= (size_t)ADJ_VERTEX_SMEM_MAX)
+        TDI_TRY(launch(b, 0, k_adj_vertex_tiled, dim3((m.V + AV_V - 1) / AV_V, (F + AV_F - 1) / AV_F), dim3(256),
+                       adj_vertex_smem(m.KP), s, m, x, F, (const double *)o.R, (const float *)d.cam, o.geo));
+    else
+        TDI_TRY(launch(b, 0, k_adj_vertex, dim3((m.V + 255) / 256, F), dim3(256), 0, s, m, x, F, (const double *)o.R,
+                       (const float *)d.cam, o.geo));
     TDI_CUDA(cudaMemsetAsync(o.img, 0, np * sizeof(double), s));
     TDI_TRY(launch(b, 0, k_adj_shade, dim3(16, F), dim3(AD_THREADS), 0, s, m, (const DBatch)d, x, lam, L, F,
                    (const double *)o.geo, (const double *)o.R, o.img));
@@ -1354,7 +1361,7 @@ tdi_status tdi_batch_loss_backward(tdi_batch *b, const tdi_fit_config *cfg, cons
                    (const double *)o.geo, (const double *)o.R, (const double *)o.adjI, o.dP0, o.dpos, o.glob));
     TDI_TRY(launch(b, 0, k_adj_vertex_back, dim3((m.V + 255) / 256, F), dim3(256), 0, s, m, F, (const double *)o.geo,
                    (const double *)o.R, (const float *)b->d.cam, (const double *)o.dpos, o.dP0, o.glob));
-    TDI_TRY(launch(b, 0, k_adj_eps, dim3((m.V + AD_VT - 1) / AD_VT, F), dim3(128), 0, s, m, F, (const double *)o.dP0,
+    TDI_TRY(launch(b, 0, k_adj_eps, dim3((m.V + AD_VT - 1) / AD_VT, (F + AE_F - 1) / AE_F), dim3(128), 0, s, m, F, (const double *)o.dP0,
                    o.geps));
     TDI_TRY(launch(b, 0, k_adj_final, dim3((F + 127) / 128), dim3(128), 0, s, m, F, (const double *)o.R,
                    (const double *)o.glob, (const double *)o.geps, gx, glam, gL));
