@@ -284,7 +284,8 @@ tdi_status set_attrs()
     TDI_CUDA(cudaFuncSetAttribute(k_vertex_t<VT_FPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_vertex_t<VT_FPT_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_barrier_full, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    TDI_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_solve_t<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    TDI_CUDA(cudaFuncSetAttribute(k_solve_t<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_precheck, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     TDI_CUDA(cudaFuncSetAttribute(k_normal_eq_tc<NE_GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
@@ -484,7 +485,8 @@ tdi_status normal_equations(const Launch &L, const Cfg &c, int stage)
     }
     TDI_TRY(launch(L.bt, KID_BARRIER, k_barrier_full, dim3(L.A()), dim3(256), L.smem_bar(), L.s, L.m, L.b,
                    (int)(stage == ST_FINETUNE)));
-    TDI_TRY(launch(L.bt, KID_SOLVE, k_solve, dim3(L.A()), dim3(SV_THREADS), L.smem_solve(), L.s, L.m, L.b, c, stage));
+    TDI_TRY(launch(L.bt, KID_SOLVE, L.m.KT <= 96 ? k_solve_t<6> : k_solve_t<8>, dim3(L.A()), dim3(SV_THREADS),
+                   L.smem_solve(), L.s, L.m, L.b, c, stage));
     return TDI_OK;
 }
 
