@@ -1979,6 +1979,8 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     __shared__ float G[4][NL];
     __shared__ float s_p[NL][3];
     __shared__ float s_v[NL][3], s_ivz[NL], s_ivz2[NL];
+    __shared__ int s_lis[NL];
+    __shared__ float s_R[9], s_dR[27];
     const int tid = threadIdx.x;
     const float *x = b.x + (size_t)f * KTP;       // the accepted point (= evaluation point)
     const float *R = b.R + f * 9, *dR = b.dR + f * 27;
@@ -1989,8 +1991,13 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
     const float fs = b.face_size[f];
     const float *bnd = b.bounds + (size_t)f * 4 * NL;
     const float *xl = b.xl + f * NL, *yl = b.yl + f * NL;
+    if (tid >= 64 && tid < 64 + 36) {
+        const int q = tid - 64;
+        if (q < 9) s_R[q] = R[q]; else s_dR[q - 9] = dR[q - 9];
+    }
     if (tid < NL) {
         const int v = m.lis[tid];
+        s_lis[tid] = v;
         const float4 pv = geo[v];
         const float p0 = pv.x, p1 = pv.y, p2 = pv.z;
         s_p[tid][0] = p0; s_p[tid][1] = p1; s_p[tid][2] = p2;
@@ -2011,40 +2018,60 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
         s_ivz2[tid] = ivz * ivz;
     }
     __syncthreads();
-    // rows of the constraint gradients: warps take landmarks, lanes take columns
-    for (int i = tid >> 5; i < NL; i += 8)
+    // rows of the constraint gradients: warps take landmarks (i = warp + 8 q), lanes take
+    // columns (a = lane + 32 c). Per column the basis values of all the warp's landmarks are
+    // loaded before any is used, so that their loads are in flight together; the rotation and
+    // its derivatives come from shared memory.
+    constexpr int BQ = (NL + 7) / 8;
+    const int warp = tid >> 5;
     for (int a = tid & 31; a < NE_P8; a += 32) {
-        const float p0 = s_p[i][0], p1 = s_p[i][1], p2 = s_p[i][2];
-        const float vx = s_v[i][0], vy = s_v[i][1], vz = s_v[i][2];
-        const float ivz = s_ivz[i], ivz2 = s_ivz2[i];
-        float wx = 0.0f, wy = 0.0f;
-        if (a < K) {
-            const float *ex = m.E + (size_t)m.lis[i] * 3 * m.KP;
-            const float RIX = ex[a], RIY = ex[m.KP + a], RIZ = ex[2 * m.KP + a];
-            const float dvx = (RIX * R[0] + RIY * R[3]) + RIZ * R[6];
-            const float dvy = (RIX * R[1] + RIY * R[4]) + RIZ * R[7];
-            const float dvz = (RIX * R[2] + RIY * R[5]) + RIZ * R[8];
-            wx = (phix * ivz2) * (dvx * vz - dvz * vx);
-            wy = (phiy * ivz2) * (dvy * vz - dvz * vy);
-        } else if (a < KT) {
-            const int cidx = a - K;
-            if (cidx == 0) { wx = phix * ivz; wy = 0.0f; }
-            else if (cidx == 1) { wx = 0.0f; wy = phiy * ivz; }
-            else if (cidx == 2) { wx = ((-phix) * vx) * ivz2; wy = ((-phiy) * vy) * ivz2; }
-            else {
-                const float *d = dR + 9 * (cidx - 3);
-                const float dvx = (d[0] * p0 + d[3] * p1) + d[6] * p2;
-                const float dvy = (d[1] * p0 + d[4] * p1) + d[7] * p2;
-                const float dvz = (d[2] * p0 + d[5] * p1) + d[8] * p2;
-                wx = (phix * ivz2) * (vz * dvx - vx * dvz);
-                wy = (phiy * ivz2) * (vz * dvy - vy * dvz);
+        float eb[BQ][3];
+#pragma unroll
+        for (int q = 0; q < BQ; ++q) {
+            const int i = warp + 8 * q;
+            eb[q][0] = eb[q][1] = eb[q][2] = 0.0f;
+            if (i < NL && a < K) {
+                const float *ex = m.E + (size_t)s_lis[i] * 3 * m.KP;
+                eb[q][0] = __ldg(ex + a);
+                eb[q][1] = __ldg(ex + m.KP + a);
+                eb[q][2] = __ldg(ex + 2 * m.KP + a);
             }
         }
-        const bool live = a < KT;
-        Fm[(0 * NL + i) * NE_P8 + a] = live ? -wx / G[0][i] : 0.0f;
-        Fm[(1 * NL + i) * NE_P8 + a] = live ? -wy / G[1][i] : 0.0f;
-        Fm[(2 * NL + i) * NE_P8 + a] = live ? wx / G[2][i] : 0.0f;
-        Fm[(3 * NL + i) * NE_P8 + a] = live ? wy / G[3][i] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < BQ; ++q) {
+            const int i = warp + 8 * q;
+            if (i >= NL) continue;
+            const float p0 = s_p[i][0], p1 = s_p[i][1], p2 = s_p[i][2];
+            const float vx = s_v[i][0], vy = s_v[i][1], vz = s_v[i][2];
+            const float ivz = s_ivz[i], ivz2 = s_ivz2[i];
+            float wx = 0.0f, wy = 0.0f;
+            if (a < K) {
+                const float RIX = eb[q][0], RIY = eb[q][1], RIZ = eb[q][2];
+                const float dvx = (RIX * s_R[0] + RIY * s_R[3]) + RIZ * s_R[6];
+                const float dvy = (RIX * s_R[1] + RIY * s_R[4]) + RIZ * s_R[7];
+                const float dvz = (RIX * s_R[2] + RIY * s_R[5]) + RIZ * s_R[8];
+                wx = (phix * ivz2) * (dvx * vz - dvz * vx);
+                wy = (phiy * ivz2) * (dvy * vz - dvz * vy);
+            } else if (a < KT) {
+                const int cidx = a - K;
+                if (cidx == 0) { wx = phix * ivz; wy = 0.0f; }
+                else if (cidx == 1) { wx = 0.0f; wy = phiy * ivz; }
+                else if (cidx == 2) { wx = ((-phix) * vx) * ivz2; wy = ((-phiy) * vy) * ivz2; }
+                else {
+                    const float *d = s_dR + 9 * (cidx - 3);
+                    const float dvx = (d[0] * p0 + d[3] * p1) + d[6] * p2;
+                    const float dvy = (d[1] * p0 + d[4] * p1) + d[7] * p2;
+                    const float dvz = (d[2] * p0 + d[5] * p1) + d[8] * p2;
+                    wx = (phix * ivz2) * (vz * dvx - vx * dvz);
+                    wy = (phiy * ivz2) * (vz * dvy - vy * dvz);
+                }
+            }
+            const bool live = a < KT;
+            Fm[(0 * NL + i) * NE_P8 + a] = live ? -wx / G[0][i] : 0.0f;
+            Fm[(1 * NL + i) * NE_P8 + a] = live ? -wy / G[1][i] : 0.0f;
+            Fm[(2 * NL + i) * NE_P8 + a] = live ? wx / G[2][i] : 0.0f;
+            Fm[(3 * NL + i) * NE_P8 + a] = live ? wy / G[3][i] : 0.0f;
+        }
     }
     __syncthreads();
     const float *lb = m.eps_b + (ft_bounds ? 2 : 0) * K;
@@ -2124,19 +2151,22 @@ __global__ void __launch_bounds__(256) k_barrier_full(DModel m, DBatch b, int ft
 //
 // The lower triangle is held in registers: thread (tr, tc) = (tid % 16, tid / 16) owns the
 // entries (i, l) with i = tr + 16a, l = tc + 16b, i >= l. Step j: every thread reads column j
-// as its owners left it in shared memory (pivot included), forms l_jj and r_j itself (the same
-// correctly rounded values everywhere) and the scaled entries it needs, and subtracts
-// L(i,j) L(l,j) from its entries right of column j; the owners of column j + 1 then store it
-// for the next step. Each entry so receives its updates in increasing j, the sequence of the
+// as its owners left it in shared memory (pivot included) and r_j as the pivot's owner formed
+// it, forms the scaled entries it needs, and subtracts L(i,j) L(l,j) from its entries right of
+// column j: the register block holding column j + 1 first, after which the owners of column
+// j + 1 store it and the owner of its pivot forms l and r for the next step while the other
+// blocks are updated. Each entry so receives its updates in increasing j, the sequence of the
 // oracle's left-looking dot products. One barrier per step; the two substitutions run in one
 // warp, four rows per lane, the newly known value broadcast by shuffle.
 //
-// The steps run in groups of 16 columns, one group per register block, with the group loop
-// unrolled. Every register block is then named by a compile-time index, and the finished blocks
-// are skipped without tests. Selecting the next column's block at run time instead moved the
-// whole block array into local memory (a 288-byte stack frame). Keeping it in registers
+// The steps run in groups of 16 columns, one group per register block, each group its own
+// instantiation. Every register block is then named by a compile-time index, and the finished
+// blocks are skipped without tests. Selecting the next column's block at run time instead moved
+// the whole block array into local memory (a 288-byte stack frame). Keeping it in registers
 // while updating every block under run-time tests measured slower still: 1.59 µs per
-// evaluation, against 1.10 µs with the stack and 0.96 µs in groups.
+// evaluation, against 1.10 µs with the stack and 0.96 µs in groups. The substitutions with the
+// reciprocals in registers and no stores inside the passes took it to 0.90 µs, and the pivot
+// formed one step ahead by its owner to 0.86 µs.
 
 constexpr int SV_THREADS = 256;
 constexpr int SV_MAXN = 128;
@@ -2147,25 +2177,106 @@ __host__ __device__ __forceinline__ size_t solve_smem(int n)
 }
 
 // One substitution pass of the warp: rows i = lane + 32 q (q < 4) start from t[q]; for each
-// step k (ascending when fwd, descending otherwise) the owner of row k forms x_k = t_k * r_k,
-// every row i after k in that order subtracts coef(i, k) x_k. Results in out[].
+// step k (ascending when FWD, descending otherwise) the owner of row k (lane k % 32) forms
+// x_k = t_k r_k from its own registers and broadcasts it, and every row i after k in that
+// order subtracts coef(i, k) x_k. The steps run in four segments of 32 with the row slot q a
+// compile-time index, and nothing is stored inside the pass, so that the coefficient loads of
+// later steps can be issued early. x of the lane's own rows ends in xm[].
 template <bool FWD>
-__device__ __forceinline__ void sv_substitute(int n, double (&t)[4], const double *Lf, const double *rv, double *out)
+__device__ __forceinline__ void sv_substitute(int n, double (&t)[4], const double (&rm)[4], double (&xm)[4],
+                                              const double *Lf)
 {
     const int lane = threadIdx.x & 31;
-    for (int s = 0; s < n; ++s) {
-        const int k = FWD ? s : n - 1 - s;
-        const int q = k >> 5;
-        const double tk = q == 0 ? t[0] : q == 1 ? t[1] : q == 2 ? t[2] : t[3];
-        const double xk = __shfl_sync(0xffffffffu, tk, k & 31) * rv[k];
-        if (lane == 0) out[k] = xk;
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-            const int i = lane + 32 * qq;
-            // forward: L(i,k) for i > k (column k); back: L(k,i) for i < k (column i)
-            if (FWD ? (i > k && i < n) : (i < k)) t[qq] -= (FWD ? Lf[(size_t)k * n + i] : Lf[(size_t)i * n + k]) * xk;
+    for (int s = 0; s < 4; ++s) {
+        const int q = FWD ? s : 3 - s;
+        if (32 * q >= n) continue;
+#pragma unroll 4
+        for (int u = 0; u < 32; ++u) {
+            const int kk = FWD ? u : 31 - u;
+            const int k = 32 * q + kk;
+            if (k >= n) { if (FWD) break; else continue; }
+            const double xo = t[q] * rm[q];             // meaningful in the owner lane
+            if (lane == kk) xm[q] = xo;
+            const double xk = __shfl_sync(0xffffffffu, xo, kk);
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                if (FWD ? qq < q : qq > q) continue;
+                const int i = lane + 32 * qq;
+                // forward: L(i,k) for i > k (column k); back: L(k,i) for i < k (column i)
+                if (FWD ? (i > k && i < n) : (i < k)) t[qq] -= (FWD ? Lf[(size_t)k * n + i] : Lf[(size_t)i * n + k]) * xk;
+            }
         }
     }
+}
+
+// The trailing update of step j (column j scaled into ci, cl), with column j + 1 in register
+// block B: the blocks (a, B) first; then the owners of column j + 1 store it, and the owner of
+// its pivot forms l = sqrt(s) and r = 1 / l (both correctly rounded) for the next step while
+// the other blocks (a, bb > B) are updated. Blocks left of B receive no more updates.
+template <int RB, int B>
+__device__ __forceinline__ void sv_update(double (&v)[RB][RB], const double (&ci)[RB], const double (&cl)[RB],
+                                          int tr, int tc, int j, int n, double *rn, double *Lf, double *rv)
+{
+#pragma unroll
+    for (int a = B; a < RB; ++a) {
+        const int i = tr + 16 * a, l = tc + 16 * B;
+        if (l > j && i >= l && i < n) v[a][B] -= ci[a] * cl[B];
+    }
+    const int jn = j + 1;
+    if (jn < n && tc == (jn & 15)) {
+#pragma unroll
+        for (int a = B; a < RB; ++a) {
+            const int i = tr + 16 * a;
+            if (i >= jn && i < n) rn[i] = v[a][B];
+        }
+        if (tr == (jn & 15)) {
+            const double sn = v[B][B];
+            if (sn > 0.0) {
+                const double ln = sqrt(sn);
+                Lf[(size_t)jn * n + jn] = ln;
+                rv[jn] = __drcp_rn(ln);
+            }
+        }
+    }
+#pragma unroll
+    for (int a = B + 1; a < RB; ++a)
+#pragma unroll
+        for (int bb = B + 1; bb <= a; ++bb) {
+            const int i = tr + 16 * a, l = tc + 16 * bb;
+            if (l > j && i >= l && i < n) v[a][bb] -= ci[a] * cl[bb];
+        }
+}
+
+// Steps j of column group J (columns 16 J .. 16 J + 15), then the next group; false when a
+// pivot is not positive (every thread reads the same pivot, so all return together). Blocks
+// left of group J (bb < J) and rows above it (a < J) are finished: their columns l < 16 J <= j
+// receive no more updates, so they are skipped statically.
+template <int RB, int J>
+__device__ __forceinline__ bool sv_factor(double (&v)[RB][RB], double *raw, double *Lf, double *rv,
+                                          int tr, int tc, int tid, int n)
+{
+    const int jend = min(n, 16 * J + 16);
+    for (int j = 16 * J; j < jend; ++j) {
+        const double *rj = raw + (j & 1) * SV_MAXN;
+        const double sj = rj[j];
+        if (!(sj > 0.0)) return false;
+        const double r = rv[j];                          // formed by the pivot's owner in step j - 1
+        if (tid > j && tid < n) Lf[(size_t)j * n + tid] = rj[tid] * r;
+        double ci[RB], cl[RB];
+#pragma unroll
+        for (int a = J; a < RB; ++a) {
+            const int i = tr + 16 * a, l = tc + 16 * a;
+            ci[a] = (i > j && i < n) ? rj[i] * r : 0.0;
+            cl[a] = (l > j && l < n) ? rj[l] * r : 0.0;
+        }
+        double *rn = raw + ((j + 1) & 1) * SV_MAXN;
+        if (j < 16 * J + 15) sv_update<RB, J>(v, ci, cl, tr, tc, j, n, rn, Lf, rv);
+        else sv_update<RB, (J + 1 < RB ? J + 1 : J)>(v, ci, cl, tr, tc, j, n, rn, Lf, rv);
+        __syncthreads();
+    }
+    if constexpr (J + 1 < RB) return sv_factor<RB, J + 1>(v, raw, Lf, rv, tr, tc, tid, n);
+    else return true;
 }
 
 template <int RB>
@@ -2194,83 +2305,43 @@ __device__ __forceinline__ void solve_frame(const DModel &m, const DBatch &b, co
 #pragma unroll
     for (int a = 0; a < RB; ++a)
         if (tc == 0 && tr + 16 * a < n) raw[tr + 16 * a] = v[a][0];
+    if (tid == 0 && v[0][0] > 0.0) {
+        const double l0 = sqrt(v[0][0]);
+        Lf[0] = l0;
+        rv[0] = __drcp_rn(l0);
+    }
     __syncthreads();
-    // Columns in register-block groups J (columns 16 J .. 16 J + 15), the group loop unrolled
-    // so that every register block is named by a compile-time index. Blocks left of group J
-    // (bb < J) and rows above it (a < J) are finished: their columns l < 16 J <= j receive no
-    // more updates, so they are skipped statically.
-#pragma unroll
-    for (int J = 0; J < RB; ++J) {
-        const int jend = min(n, 16 * J + 16);
-        for (int j = 16 * J; j < jend; ++j) {
-            const double *rj = raw + (j & 1) * SV_MAXN;
-            const double sj = rj[j];
-            if (!(sj > 0.0)) {                           // block-uniform: every thread read the same pivot
-                float *d = b.d + (size_t)f * KTP;
-                for (int i = tid; i < n; i += SV_THREADS) d[i] = __int_as_float(0x7fc00000);
-                if (tid == 0) {
-                    ctl.flags |= FLAG_CHOL_FAILED | FLAG_NAN_DIRECTION;
-                    end_shape_stage(c, ctl, stage, ctl.outer);
-                }
-                return;
-            }
-            const double ljj = sqrt(sj), r = 1.0 / ljj;
-            if (tid == 0) { Lf[(size_t)j * n + j] = ljj; rv[j] = r; }
-            if (tid > j && tid < n) Lf[(size_t)j * n + tid] = rj[tid] * r;
-            // trailing update of the owned entries right of column j
-            double ci[RB], cl[RB];
-#pragma unroll
-            for (int a = J; a < RB; ++a) {
-                const int i = tr + 16 * a, l = tc + 16 * a;
-                ci[a] = (i > j && i < n) ? rj[i] * r : 0.0;
-                cl[a] = (l > j && l < n) ? rj[l] * r : 0.0;
-            }
-#pragma unroll
-            for (int a = J; a < RB; ++a)
-#pragma unroll
-                for (int bb = J; bb <= a; ++bb) {
-                    const int i = tr + 16 * a, l = tc + 16 * bb;
-                    if (l > j && i >= l && i < n) v[a][bb] -= ci[a] * cl[bb];
-                }
-            // the next column before its scaling, pivot included: register block J, or J + 1
-            // when column j closes the group
-            const int jn = j + 1;
-            if (jn < n && tc == (jn & 15)) {
-                double *rn = raw + (jn & 1) * SV_MAXN;
-                if (jn < 16 * J + 16) {
-#pragma unroll
-                    for (int a = J; a < RB; ++a) {
-                        const int i = tr + 16 * a;
-                        if (i >= jn && i < n) rn[i] = v[a][J];
-                    }
-                } else if (J + 1 < RB) {
-#pragma unroll
-                    for (int a = J + 1; a < RB; ++a) {
-                        const int i = tr + 16 * a;
-                        if (i >= jn && i < n) rn[i] = v[a][J + 1 < RB ? J + 1 : J];
-                    }
-                }
-            }
-            __syncthreads();
+    // Columns in register-block groups J (columns 16 J .. 16 J + 15), one instantiation per
+    // group, so that every register block is named by a compile-time index.
+    if (!sv_factor<RB, 0>(v, raw, Lf, rv, tr, tc, tid, n)) {    // block-uniform: the same pivot everywhere
+        float *d = b.d + (size_t)f * KTP;
+        for (int i = tid; i < n; i += SV_THREADS) d[i] = __int_as_float(0x7fc00000);
+        if (tid == 0) {
+            ctl.flags |= FLAG_CHOL_FAILED | FLAG_NAN_DIRECTION;
+            end_shape_stage(c, ctl, stage, ctl.outer);
         }
+        return;
     }
     // forward and back substitution in one warp
     if (tid < 32) {
-        double t[4];
+        double t[4], rm[4], xm[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int i = tid + 32 * q;
             t[q] = i < n ? (double)gv[i] : 0.0;
+            rm[q] = i < n ? rv[i] : 0.0;
+            xm[q] = 0.0;
         }
-        sv_substitute<true>(n, t, Lf, rv, yv);
+        sv_substitute<true>(n, t, rm, xm, Lf);
         // y_i = t_i r_i: the value the owner of row i broadcast at step i
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = xm[q];
+        sv_substitute<false>(n, t, rm, xm, Lf);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int i = tid + 32 * q;
-            t[q] = i < n ? t[q] * rv[i] : 0.0;
+            if (i < n) yv[i] = xm[q];
         }
-        __syncwarp();
-        sv_substitute<false>(n, t, Lf, rv, yv);
     }
     __syncthreads();
     const double y = tid < n ? yv[tid] : 0.0;

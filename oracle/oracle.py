@@ -2,8 +2,10 @@
 
 Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use this
 module, always as the checker or the timed CPU baseline -- never as part of the product.
-Parity of this restatement is unpinned: 3DI ships no golden vectors for this path and its
-sources need OpenCV to build.
+3DI ships no golden vectors for this path, so the restatement is pinned to the reference
+itself. Its hot-path CUDA sources are built as they lie into ``oracle/_ref/`` (``ref.mk``,
+with stand-in headers for the OpenCV display helpers that the path never calls), and
+``tests/test_ref_pinning.py`` compares this oracle with them stage by stage on a B200.
 """
 from __future__ import annotations
 
@@ -282,6 +284,41 @@ def apply_identity(mean0, id_basis, alpha, tex0, tex_basis, beta):
     tex = np.zeros(V, np.float32)
     lib("f32").o_apply_identity(V, KA, KB, _p(mean0), _p(I), _p(a), _p(tex0), _p(T), _p(b), _p(mean), _p(tex))
     return mean, tex
+
+
+def solve_shape(H, g, damping=0.0):
+    """The shape solve's arithmetic (solve_shape in tdi_oracle.c) restated in numpy float64,
+    which rounds every product and difference on its own. The factor is read from the upper
+    triangle of H: entry (i, l), i >= l, at H[l, i], with the damping added on the diagonal.
+    Pivots have reciprocals r_j = 1 / sqrt(s_j). Each entry's updates L(i,k) L(l,k) are
+    subtracted in increasing k. Here they run column by column, which gives each entry the
+    same sequence as the C file's dot products. Forward and back substitution take their terms
+    in increasing and decreasing k. Returns d = -x as float32, or None when a pivot is not
+    positive."""
+    Hu = np.triu(np.asarray(H, np.float64))
+    A = Hu + np.triu(Hu, 1).T
+    n = A.shape[0]
+    A[np.arange(n), np.arange(n)] += float(np.float32(damping))
+    L = np.zeros((n, n))
+    r = np.zeros(n)
+    for j in range(n):
+        s = A[j, j]
+        if not s > 0.0:
+            return None
+        r[j] = 1.0 / np.sqrt(s)
+        c = A[j + 1:, j] * r[j]
+        L[j + 1:, j] = c
+        A[j + 1:, j + 1:] -= np.outer(c, c)
+    t = np.asarray(g, np.float64).copy()
+    y = np.zeros(n)
+    for k in range(n):
+        y[k] = t[k] * r[k]
+        t[k + 1:] -= L[k + 1:, k] * y[k]
+    t = y.copy()
+    for k in range(n - 1, -1, -1):
+        y[k] = t[k] * r[k]
+        t[:k] -= L[k, :k] * y[k]
+    return (-y).astype(np.float32)
 
 
 def max_threads(kind="f32") -> int:

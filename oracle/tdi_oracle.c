@@ -2,7 +2,8 @@
  * CPU oracle for the 3DI per-frame fitting path -- TEST INFRASTRUCTURE ONLY (see
  * tdi_oracle.h). Restates, operation by operation, the reference CUDA sources of
  * Computational-Psychiatry/3DI; each function names the file:line it follows.
- * PARITY UNPINNED: the reference has no golden vectors and cannot be built here.
+ * Parity is pinned to the reference's own kernels, built from its sources by ref.mk into
+ * _ref/ and compared stage by stage in tests/test_ref_pinning.py.
  *
  * Arithmetic definitions (identical in the product's CUDA kernels):
  *  - elementwise formulas: IEEE arithmetic in REAL, no FMA contraction, the operand order

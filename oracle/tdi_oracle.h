@@ -11,9 +11,11 @@
  *                         drawn) is decided in FP32 on FP32-rounded projections in both
  *                         builds, so the two share their discrete structure.
  *
- * Parity status: the reference ships no tests, golden vectors or fixtures for this path
- * and cannot be built here (it needs OpenCV), so this restatement is PARITY UNPINNED.
- * Every function cites the reference file:line it restates.
+ * Parity status: the reference ships no tests, golden vectors or fixtures for this path, so
+ * the restatement is pinned to the reference itself. ref.mk builds its hot-path CUDA sources
+ * as they lie into _ref/, with stand-in headers for the OpenCV display helpers that the path
+ * never calls. tests/test_ref_pinning.py compares the two stage by stage on a B200. Every
+ * function cites the reference file:line it restates.
  *
  * Layouts (shared with the product's C ABI, include/tdi.h):
  *   images     256x256 float, column-major: pixel (x, y) at x*256 + y

@@ -127,3 +127,33 @@ def test_damped_solve_matches_oracle(tdi, synth, O, small_case):
         assert rep[i].flags == orep[i].flags and rep[i].iters_rigid == orep[i].iters_rigid
         err = np.abs(x[i] - ox[i]) / np.maximum(np.abs(ox[i]), 1e-2)
         assert err.max() <= 1e-5, err.max()
+
+
+@pytest.mark.parametrize("n_expr,mode", [(79, "exact"), (100, "tensor")])
+def test_shape_solve_bit_exact_for_both_register_layouts(tdi, synth, O, n_expr, mode):
+    """The shape solve holds the factor in 6 x 6 register blocks for up to 96 unknowns and in
+    8 x 8 blocks up to 128 (reached with the tensor-core normal equations and more than 90
+    expression components). Both give the oracle's solve of the H and g they were handed, bit
+    for bit (oracle.solve_shape, pinned to the C oracle on the CPU)."""
+    tdi.require_gpu()
+    F = 2
+    m = synth.make_model(5000, 9800, 0, n_expr=n_expr)
+    fr = synth.make_frames(m, F, 0, image_wh=(256, 256), tz=0.6)
+    model = tdi.Model(m)
+    batch = tdi.Batch(model, F)
+    L = np.full(F, synth.L_INTENSITY, np.float32)
+    fr.target = np.zeros((F, tdi.NPIX), np.float32)
+    batch.set_frames(fr)
+    batch.set_state(fr.state_true, fr.lam_true, L)
+    img, _ = batch.render()
+    fr.target = synth.add_noise(img, 0.02, 0)
+    batch.set_frames(fr)
+    batch.set_state(fr.state_init, np.tile(synth.LAMBDA_INIT, (F, 1)), L)
+    neq = tdi.NORMAL_EQ_TENSOR if mode == "tensor" else tdi.NORMAL_EQ_EXACT
+    batch.evaluate(tdi.default_config(normal_eq=neq))
+    for i in range(F):
+        ne = batch.read(i, tdi.READ_NORMAL_EQ)
+        assert ne["H"].shape == (n_expr + 6, n_expr + 6)
+        d = O.solve_shape(ne["H"], ne["g"])
+        assert d is not None
+        np.testing.assert_array_equal(ne["d"], d)

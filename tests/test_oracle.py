@@ -239,3 +239,15 @@ def test_damped_direction_solves_the_shifted_system(synth, O, small_case):
         r = H @ e["d"].astype(np.float64) + e["g"].astype(np.float64)
         assert np.linalg.norm(r) <= 1e-4 * np.linalg.norm(e["g"])
     assert np.array_equal(O.evaluate(om, fs, 0, O.config(damping=0.0), fr.state_init[0], lam, L)["d"], e0["d"])
+
+
+def test_numpy_shape_solve_equals_the_oracles(synth, O, small_case):
+    """oracle.solve_shape (the solve restated in numpy float64, the checker of the GPU solve for
+    models the oracle's evaluation is slow on) gives the C oracle's direction bit for bit on
+    the H and g that the oracle returns, undamped and damped."""
+    m, fr, om = small_case
+    fs = O.FrameSet(fr)
+    for damp in (0.0, 1e3):
+        e = O.evaluate(om, fs, 0, O.config(damping=damp), fr.state_init[0], synth.LAMBDA_INIT,
+                       float(synth.L_INTENSITY))
+        np.testing.assert_array_equal(O.solve_shape(e["H"], e["g"], damp), e["d"])
