@@ -740,6 +740,7 @@ constexpr int RD_BLOCKS = 16;               // depth pass: blocks per frame (at 
 constexpr int RD_MAX_BLOCKS = 256;          // depth pass: blocks per frame when few frames render
 constexpr int RR_THREADS = 1024;            // resolve: one block per frame
 constexpr int RR_WARPS = RR_THREADS / 32;
+constexpr int RR_ILP = 2;                  // resolve: listed entries per lane in flight together
 
 __global__ void __launch_bounds__(RD_THREADS) k_raster_depth(DModel m, DBatch b)
 {
@@ -886,29 +887,80 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
         return idx;
     };
     uint32_t cnt[NTMP] = {0, 0, 0, 0};
-    for (int base = e_begin; base < e_end; base += 32) {
-        const int e = base + lane;
-        bool sv[NTMP] = {false, false, false, false};
-        bool own[NTMP] = {false, false, false, false};
-        uint32_t pix[NTMP] = {0, 0, 0, 0};
-        float al[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f}, be[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f};
-        int idx = -1;
-        if (e < e_end) idx = evaluate(e, sv, own, pix, al, be);
+    if (one_pass) {
+        // RR_ILP entries per lane and step (entries base + 32 h + lane), in phases: all their
+        // triangles' corners, all sample sets, all z-buffer keys, then the survivors entry by
+        // entry in entry order, so that the dependent loads of the entries overlap
+        for (int base = e_begin; base < e_end; base += 32 * RR_ILP) {
+            int idx[RR_ILP];
+            int4 tq[RR_ILP];
+            float4 pb[RR_ILP], pc[RR_ILP], pa[RR_ILP];
 #pragma unroll
-        for (int r = 0; r < NTMP; ++r) {
-            const unsigned msk = __ballot_sync(0xffffffffu, sv[r]);
-            if (one_pass && sv[r]) {
-                Fragment fr;
-                fr.pix_owner = pix[r] | (own[r] ? 0x80000000u : 0u);
-                fr.tri = idx;
-                fr.al = al[r];
-                fr.be = be[r];
-                wstage[(size_t)r * per_e + cnt[r] + __popc(msk & lt_mask)] = fr;
-                const int px = (int)(pix[r] >> 8), py = (int)(pix[r] & 255);
-                bx0 = min(bx0, px); bx1 = max(bx1, px);
-                by0 = min(by0, py); by1 = max(by1, py);
+            for (int h = 0; h < RR_ILP; ++h) {
+                const int e = base + 32 * h + lane;
+                idx[h] = e < e_end ? __ldcg(list + e) : -1;
             }
-            cnt[r] += __popc(msk);
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) tq[h] = __ldg(m.tl4 + (idx[h] >= 0 ? idx[h] : 0));
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) {
+                pb[h] = __ldg(pj + tq[h].x);
+                pc[h] = __ldg(pj + tq[h].y);
+                pa[h] = __ldg(pj + tq[h].z);
+            }
+            uint32_t pix[RR_ILP][NTMP];
+            float al[RR_ILP][NTMP], be[RR_ILP][NTMP];
+            int nf[RR_ILP];
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) {
+                nf[h] = 0;
+                if (idx[h] >= 0) {
+                    uint32_t fl2 = 0;
+                    nf[h] = tri_samples(pb[h].x, pb[h].y, pc[h].x, pc[h].y, pa[h].x, pa[h].y, x0, y0, fl2,
+                                        [&](int r, uint32_t px, float a, float bb) {
+                                            pix[h][r] = px; al[h][r] = a; be[h][r] = bb;
+                                        });
+                }
+            }
+            unsigned long long key[RR_ILP][NTMP];
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h)
+#pragma unroll
+                for (int r = 0; r < NTMP; ++r) key[h][r] = r < nf[h] ? __ldcg(zb + pix[h][r]) : 0ull;
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) {
+                const uint32_t zbits = __float_as_uint(pb[h].z) & 0x7FFFFFFFu;
+                const unsigned long long mykey = zkey(tag, pb[h].z, idx[h]);
+#pragma unroll
+                for (int r = 0; r < NTMP; ++r) {
+                    const bool sv = r < nf[h] && survives(key[h][r], tag, zbits) && !(r == 0 && idx[h] == 0);
+                    const unsigned msk = __ballot_sync(0xffffffffu, sv);
+                    if (sv) {
+                        Fragment fr;
+                        fr.pix_owner = pix[h][r] | (key[h][r] == mykey ? 0x80000000u : 0u);
+                        fr.tri = idx[h];
+                        fr.al = al[h][r];
+                        fr.be = be[h][r];
+                        wstage[(size_t)r * per_e + cnt[r] + __popc(msk & lt_mask)] = fr;
+                        const int px = (int)(pix[h][r] >> 8), py = (int)(pix[h][r] & 255);
+                        bx0 = min(bx0, px); bx1 = max(bx1, px);
+                        by0 = min(by0, py); by1 = max(by1, py);
+                    }
+                    cnt[r] += __popc(msk);
+                }
+            }
+        }
+    } else {
+        // counts only; the survivors are formed again in the write pass
+        for (int base = e_begin; base < e_end; base += 32) {
+            const int e = base + lane;
+            bool sv[NTMP] = {false, false, false, false};
+            bool own[NTMP] = {false, false, false, false};
+            uint32_t pix[NTMP] = {0, 0, 0, 0};
+            float al[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f}, be[NTMP] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (e < e_end) evaluate(e, sv, own, pix, al, be);
+#pragma unroll
+            for (int r = 0; r < NTMP; ++r) cnt[r] += __popc(__ballot_sync(0xffffffffu, sv[r]));
         }
     }
     if (lane == 0)
