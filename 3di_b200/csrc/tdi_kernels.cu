@@ -723,6 +723,28 @@ __device__ __forceinline__ int tri_fragments(const DModel &m, const float *xp, c
     return tri_fragments_t(m, [&](int v) { return make_float2(xp[v], yp[v]); }, idx, x0, y0, pix, al, be, flags);
 }
 
+// The geometry terms of a fragment's shading: unit normal of its triangle and barycentric
+// point p in model coordinates, interpolated albedo t (corners b, c, a as geometry records).
+__device__ __forceinline__ void shade_geometry(const float4 &gb, const float4 &gc, const float4 &ga4, float al,
+                                               float be, float (&nn)[3], float (&p)[3], float &t)
+{
+    const float ga = (1 - al) - be;
+    const float b0x = gb.x, b0y = gb.y, b0z = gb.z;
+    const float c0x = gc.x, c0y = gc.y, c0z = gc.z;
+    const float a0x = ga4.x, a0y = ga4.y, a0z = ga4.z;
+    const float n_vx = b0x - a0x, n_vy = b0y - a0y, n_vz = b0z - a0z;
+    const float n_wx = c0x - a0x, n_wy = c0y - a0y, n_wz = c0z - a0z;
+    const float nrx = n_vy * n_wz - n_vz * n_wy;
+    const float nry = n_vz * n_wx - n_vx * n_wz;
+    const float nrz = n_vx * n_wy - n_vy * n_wx;
+    const float normn = sqrtf((nrx * nrx + nry * nry) + nrz * nrz);
+    nn[0] = nrx / normn; nn[1] = nry / normn; nn[2] = nrz / normn;
+    p[0] = (b0x * al + c0x * be) + a0x * ga;
+    p[1] = (b0y * al + c0y * be) + a0y * ga;
+    p[2] = (b0z * al + c0z * be) + a0z * ga;
+    t = (gb.w * al + gc.w * be) + ga4.w * ga;
+}
+
 __device__ __forceinline__ unsigned long long zkey(uint32_t tag, float Z, int tri)
 {
     return ((unsigned long long)tag << (31 + TRI_BITS)) |
@@ -1043,6 +1065,45 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
         atomicMin(&s_bbox[2], by0); atomicMax(&s_bbox[3], by1);
     }
     __syncthreads();
+    // Shading inputs of every fragment for the renders of this raster: unit normal and n . p
+    // (shc), interpolated albedo (sht), formed by shade_geometry as shade() forms them, so that
+    // the renders shade from coalesced records instead of gathering the triangle corners (R,
+    // tau and the light enter per render). RR_ILP fragments per thread have their loads in
+    // flight together. (A separate kernel of 8 blocks per frame measured slower: 38.7 us per
+    // launch against the 28 us this adds to the resolve, whose other phases it overlaps.)
+    if (!(s_flags & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW))) {
+        const int Nf = (int)min(s_row[NTMP], (uint32_t)NMAX);
+        const float4 *geo = b.geo + (size_t)f * m.V;
+        float4 *shc = b.shc + (size_t)f * NMAX;
+        float *sht = b.sht + (size_t)f * NMAX;
+        for (int p0 = tid; p0 < Nf; p0 += RR_THREADS * RR_ILP) {
+            Fragment fr[RR_ILP];
+            int4 tq[RR_ILP];
+            float4 gb[RR_ILP], gc[RR_ILP], ga[RR_ILP];
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) {
+                const int p = p0 + h * RR_THREADS;
+                fr[h] = p < Nf ? out[p] : Fragment{0u, 0, 0.0f, 0.0f};
+            }
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) tq[h] = __ldg(m.tl4 + fr[h].tri);
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) {
+                gb[h] = geo[tq[h].x];
+                gc[h] = geo[tq[h].y];
+                ga[h] = geo[tq[h].z];
+            }
+#pragma unroll
+            for (int h = 0; h < RR_ILP; ++h) {
+                const int p = p0 + h * RR_THREADS;
+                if (p >= Nf) continue;
+                float nn[3], pp[3], t;
+                shade_geometry(gb[h], gc[h], ga[h], fr[h].al, fr[h].be, nn, pp, t);
+                shc[p] = make_float4(nn[0], nn[1], nn[2], (nn[0] * pp[0] + nn[1] * pp[1]) + nn[2] * pp[2]);
+                sht[p] = t;
+            }
+        }
+    }
     if (epoch == TAG_MAX) {
         // tag range used up: the next raster starts from a cleared z-buffer
         for (int p = tid; p < NPIX; p += RR_THREADS) zb[p] = ~0ull;
@@ -1052,7 +1113,7 @@ __global__ void __launch_bounds__(RR_THREADS) k_raster_resolve(DModel m, DBatch 
         ctl.epoch = epoch == TAG_MAX ? 0u : epoch;
         ctl.flags |= fl;
         ctl.renders += 1;
-        ctl.shade_cached = 0;
+        ctl.shade_cached = (fl & (FLAG_RENDER_SKIPPED | FLAG_OVERFLOW)) ? 0 : 1;
         for (int q = 0; q < 4; ++q) ctl.bbox[q] = s_bbox[q];
         if (s_bbox[1] >= 0 && (s_bbox[0] < 1 || s_bbox[1] > DIM - 2 || s_bbox[2] < 1 || s_bbox[3] > DIM - 2))
             ctl.flags |= FLAG_OUT_OF_DOMAIN;
@@ -1091,23 +1152,14 @@ __device__ __forceinline__ Shading shade(const DModel &m, const float4 *geo, con
     const float b0x = gb.x, b0y = gb.y, b0z = gb.z;
     const float c0x = gc.x, c0y = gc.y, c0z = gc.z;
     const float a0x = ga4.x, a0y = ga4.y, a0z = ga4.z;
-    const float n_vx = b0x - a0x, n_vy = b0y - a0y, n_vz = b0z - a0z;
-    const float n_wx = c0x - a0x, n_wy = c0y - a0y, n_wz = c0z - a0z;
-    const float nrx = n_vy * n_wz - n_vz * n_wy;
-    const float nry = n_vz * n_wx - n_vx * n_wz;
-    const float nrz = n_vx * n_wy - n_vy * n_wx;
-    const float normn = sqrtf((nrx * nrx + nry * nry) + nrz * nrz);
     Shading s;
-    s.nn[0] = nrx / normn; s.nn[1] = nry / normn; s.nn[2] = nrz / normn;
-    s.p[0] = (b0x * al + c0x * be) + a0x * ga;
-    s.p[1] = (b0y * al + c0y * be) + a0y * ga;
-    s.p[2] = (b0z * al + c0z * be) + a0z * ga;
+    float t;
+    shade_geometry(gb, gc, ga4, al, be, s.nn, s.p, t);
     const float d0 = lam[0] - tau[0], d1 = lam[1] - tau[1], d2 = lam[2] - tau[2];
     float Id = (s.nn[0] * ((R[0] * d0 + R[1] * d1) + R[2] * d2)
                 + s.nn[1] * ((R[3] * d0 + R[4] * d1) + R[5] * d2))
                + s.nn[2] * ((R[6] * d0 + R[7] * d1) + R[8] * d2);
     Id = Id - ((s.nn[0] * s.p[0] + s.nn[1] * s.p[1]) + s.nn[2] * s.p[2]);
-    const float t = (gb.w * al + gc.w * be) + ga4.w * ga;
     s.t = t;
     s.tex = t + (Lint * t) * Id;
     s.Id = Id;
@@ -1183,13 +1235,13 @@ __device__ __forceinline__ void render_region(const DModel &m, const DBatch &b, 
     const float Lint = b.Lint[f];
     const Fragment *frags = b.frag + (size_t)f * NMAX;
     auto at = [&](int p) { return ((p >> 8) - rx0) * ph + KRAD + ((p & 255) - ry0); };
-    if (stage == ST_LAMBDA) {
-        // The light fit moves only the light: the geometry and so each fragment's unit normal,
-        // n . p and interpolated albedo stay those of the stage's raster. The first render
-        // after that raster forms them for every fragment (kept for this and for
-        // k_lambda_jac); later renders form only the rotated light R^T (lambda - tau), once,
-        // and the same FP32 operations as shade(): Id = (n0 q0 + n1 q1) + n2 q2 - n.p,
-        // I = t + (L t) Id.
+    if (stage == ST_LAMBDA || ctl.shade_cached) {
+        // Each fragment's unit normal, n . p and interpolated albedo depend only on the geometry
+        // of the raster: the resolve forms them (shc, sht) for every raster that renders, and
+        // the light fit, which moves only the light, keeps them for all its renders and for
+        // k_lambda_jac (a render that finds them missing forms them itself). A render forms
+        // only the rotated light R^T (lambda - tau), once, and the same FP32 operations as
+        // shade(): Id = (n0 q0 + n1 q1) + n2 q2 - n.p, I = t + (L t) Id.
         float4 *shc = b.shc + (size_t)f * NMAX;
         float *sht = b.sht + (size_t)f * NMAX;
         const bool cached = ctl.shade_cached != 0;

@@ -170,11 +170,13 @@ def algorithmic_bytes(kernel: str, V: int, T: int, K: int, n_frag: float):
         return 16.0 * V + 16.0 * T + 8.0 * n_frag, 0.0
     if kernel == "raster_resolve":
         # the frame's triangle mask, the corners and projections of the triangles with
-        # fragments (about one per fragment), their depth keys and the fragment records written
-        return T / 8.0 + n_frag * (16 + 3 * 16 + 8 + 16), 0.0
+        # fragments (about one per fragment), their depth keys and the fragment records written;
+        # then per fragment its record, its triangle's corners, three vertices' object
+        # coordinates and albedo, and the shading records written (unit normal and n . p, albedo)
+        return T / 8.0 + n_frag * (16 + 3 * 16 + 8 + 16) + n_frag * (16 + 16 + 3 * 16 + 20), 0.0
     if kernel == "render":
-        # fragments, three vertices' object coordinates and albedo, four target pixels, gradients
-        return n_frag * (16 + 3 * 16 + 4 * 4 + 5 * 4), 0.0
+        # fragments, their shading records, four target pixels, gradients
+        return n_frag * (16 + 20 + 4 * 4 + 5 * 4), 0.0
     if kernel == "neighbours":
         # fragment pixels in, four neighbour indices out
         return n_frag * (16 + 16), 0.0
