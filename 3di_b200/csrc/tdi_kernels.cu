@@ -1208,6 +1208,7 @@ constexpr int RENDER_THREADS = 512;
 constexpr int RENDER_SMEM_FLOATS = 27 * 1024;     // padded region buffers (108 KB): two blocks per SM
 constexpr int RENDER_U = 2;                       // fragments whose gathers are in flight together
 constexpr int RENDER_GU = 2;                      // the same in the gradient pass (8 loads each)
+constexpr int RENDER_SU = 4;                      // the same when shading from the resolve's terms
 constexpr int RIMG = 2 * DIM * (DIM + 2 * KRAD);  // per-frame floats of the global fallback
 
 __host__ __device__ __forceinline__ int region_floats(int rw, int rh)
@@ -1249,21 +1250,39 @@ __device__ __forceinline__ void render_region(const DModel &m, const DBatch &b, 
         const float q0 = (R[0] * d0 + R[1] * d1) + R[2] * d2;
         const float q1 = (R[3] * d0 + R[4] * d1) + R[5] * d2;
         const float q2 = (R[6] * d0 + R[7] * d1) + R[8] * d2;
+        if (cached) {
+            // RENDER_SU fragments per thread: each one's pixel word and shading terms are loaded
+            // together (the terms are indexed by the fragment, not by its contents)
+            for (int n0 = tid; n0 < N; n0 += RENDER_THREADS * RENDER_SU) {
+                uint32_t po[RENDER_SU];
+                float4 sn[RENDER_SU];
+                float t[RENDER_SU];
+#pragma unroll
+                for (int u = 0; u < RENDER_SU; ++u) {
+                    const int n = n0 + u * RENDER_THREADS;
+                    po[u] = 0u;
+                    if (n < N) {
+                        po[u] = frags[n].pix_owner;
+                        sn[u] = shc[n];
+                        t[u] = sht[n];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RENDER_SU; ++u)
+                    if (po[u] & 0x80000000u) {
+                        const float Id = ((sn[u].x * q0 + sn[u].y * q1) + sn[u].z * q2) - sn[u].w;
+                        A[at(po[u] & 0xFFFF)] = t[u] + (Lint * t[u]) * Id;
+                    }
+            }
+        } else
         for (int n = tid; n < N; n += RENDER_THREADS) {
             const Fragment fr = frags[n];
-            float4 sn;
-            float t;
-            if (cached) {
-                if (!(fr.pix_owner & 0x80000000u)) continue;
-                sn = shc[n];
-                t = sht[n];
-            } else {
-                const Shading s = shade(m, geo, fr, R, tau, lam, Lint);
-                sn = make_float4(s.nn[0], s.nn[1], s.nn[2], (s.nn[0] * s.p[0] + s.nn[1] * s.p[1]) + s.nn[2] * s.p[2]);
-                t = s.t;
-                shc[n] = sn;
-                sht[n] = t;
-            }
+            const Shading s = shade(m, geo, fr, R, tau, lam, Lint);
+            const float4 sn = make_float4(s.nn[0], s.nn[1], s.nn[2],
+                                          (s.nn[0] * s.p[0] + s.nn[1] * s.p[1]) + s.nn[2] * s.p[2]);
+            const float t = s.t;
+            shc[n] = sn;
+            sht[n] = t;
             if (fr.pix_owner & 0x80000000u) {
                 const float Id = ((sn.x * q0 + sn.y * q1) + sn.z * q2) - sn.w;
                 A[at(fr.pix_owner & 0xFFFF)] = t + (Lint * t) * Id;
